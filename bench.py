@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark of the conflict-graph hot path: ED pair tests per second.
+
+One step = build the conflict graph of one job (all pairs i<j, edge iff
+Levenshtein < editDist) into an upper CSR in HBM.  Default workload: the single
+large job -- all 262,144 codewords of the GF(4) [12,9,3] code plus the seeded
+coset vector, filtered (maxRun 3, GC [0.3,0.7]) to 207,432 words, editDist 4:
+21.5e9 pair tests and 18.6e6 edges per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+* value     -- pair tests/s with the words already in HBM (device timeline,
+               CUDA events on the library's stream; L2 flushed between steps).
+* e2e       -- the same metric through the public API with host buffers: each
+               step uploads the words from pinned memory and downloads the CSR
+               into pinned memory (wall clock around the synchronous calls).
+* roofline  -- the pair-test kernel against the INT32 issue peak (SMs x 128
+               lanes x max SM clock); algorithmic work = 16*L integer ops per
+               pair test.
+* cpu_baseline -- the reference's own CPU FillAdjList (oracle/_ref, built from
+               the reference sources) on all host cores, on a seeded sample.
+* --impl reference -- times only that reference CPU path (rank 0).
+Multi-GPU: every rank solves its own replica (the path has no exchange step);
+value = all ranks' pair tests / max-over-ranks time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from indexgen_b200 import workloads as W  # noqa: E402
+
+METRIC = "ED pair tests/s"
+UNIT = "Gpair/s"
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
+
+
+def workload(name: str):
+    if name == "linear12":
+        return dict(name="linear12_gf4_coset", desc="[12,9,3] GF(4) code + coset (seed 20251203), maxRun 3, "
+                    "GC [0.3,0.7]", words=W.linear12_candidates(), L=12, min_ed=4)
+    if name == "uniform11":
+        return dict(name="uniform11", desc="20,000 uniform n=11 (seed 12345), maxRun 3, GC [0.3,0.7]",
+                    words=W.uniform11_candidates(), L=11, min_ed=3)
+    if name == "vt16":
+        return dict(name="vt16_1M", desc="1,000,000 VT-style n=16 words (seed 16), maxRun 3, GC [0.3,0.7]",
+                    words=W.vt16_words(1_000_000, seed=16), L=16, min_ed=5)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def pairs_of(n: int) -> int:
+    return n * (n - 1) // 2
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------- clocks ----
+class ClockSampler:
+    FIELDS = ("index,pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.lines = []
+        self.t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.t:
+            self.t.join(timeout=2)
+        rows = [l.split(", ") for l in self.lines if l.count(",") >= 9]
+        mine = [r for r in rows if self.bus_id and self.bus_id in r[1].lower()] or rows
+        sm = [float(r[2]) for r in mine if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in mine if r[3].replace(".", "").isdigit()]
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in mine:
+            for name, v in zip(names, r[6:10]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(mine)}
+
+
+# ----------------------------------------------------------- cpu baseline ---
+def write_strings(path, words, L):
+    with open(path, "w") as f:
+        f.write("\n".join(W.to_strings(words, L)) + "\n")
+
+
+def ref_time(words, L, d, threads) -> dict:
+    with tempfile.TemporaryDirectory() as tmp:
+        p = os.path.join(tmp, "cands.txt")
+        write_strings(p, words, L)
+        out = subprocess.run([REF_DRIVER, "time", p, str(d), str(threads)], check=True, capture_output=True,
+                             text=True, cwd=tmp).stdout
+    return json.loads([l for l in out.splitlines() if l.startswith("{")][-1])
+
+
+def port_time(words, L, d, threads) -> dict:
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    rp, _ = O.conflict_upper(words, L, d, threads)
+    s = time.perf_counter() - t0
+    return {"N": len(words), "pairs": pairs_of(len(words)), "ones": int(2 * rp[-1]), "seconds": s,
+            "threads": threads}
+
+
+def cpu_sample(wl, target_s: float, seed: int = 1234):
+    """Seeded random subset of the workload whose CPU build takes ~target_s."""
+    words, L, d = wl["words"], wl["L"], wl["min_ed"]
+    cores = host_cores()
+    kind = "reference" if os.path.exists(REF_DRIVER) else "port"
+    timer = ref_time if kind == "reference" else port_time
+    rng = np.random.default_rng(seed)
+    m0 = min(len(words), 6000)
+    idx = np.sort(rng.choice(len(words), m0, replace=False))
+    r0 = timer(words[idx], L, d, cores)
+    rate = r0["pairs"] / max(r0["seconds"], 1e-3)
+    m = int(min(len(words), max(m0, (2 * rate * target_s) ** 0.5)))
+    idx = np.sort(rng.choice(len(words), m, replace=False))
+    return kind, timer, words[idx], cores
+
+
+def cpu_baseline(wl, target_s: float = 15.0) -> dict:
+    kind, timer, sample, cores = cpu_sample(wl, target_s)
+    r = timer(sample, wl["L"], wl["min_ed"], cores)
+    v = r["pairs"] / r["seconds"] / 1e9
+    who = "reference FillAdjList (oracle/_ref, built from the reference sources)" if kind == "reference" else \
+        "C oracle port of FillAdjList"
+    return {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{who}: seeded random subset of {len(sample)} of the {len(wl['words'])} words "
+                      f"({r['pairs']} pair tests, {r['seconds']:.2f} s, {r['ones'] // 2} edges)"}
+
+
+# ------------------------------------------------------------- reference ----
+def run_reference(args, wl, rank):
+    if rank != 0:
+        return
+    kind, timer, sample, cores = cpu_sample(wl, target_s=4.0)
+    for _ in range(args.warmup):
+        timer(sample, wl["L"], wl["min_ed"], cores)
+    secs = []
+    for _ in range(args.steps):
+        r = timer(sample, wl["L"], wl["min_ed"], cores)
+        secs.append(r["seconds"])
+    v = r["pairs"] * len(secs) / sum(secs) / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(secs) / len(secs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "n": len(wl["words"]), "L": wl["L"],
+                   "min_ed": wl["min_ed"], "pairs_per_step": r["pairs"], "sample_n": len(sample)},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"seeded random subset of {len(sample)} of {len(wl['words'])} words per step "
+                                   f"({r['pairs']} pair tests), FillAdjList with {cores} threads"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ ours ----
+def profile_traffic(wl_name):
+    """dram bytes per pair-kernel launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"pair_kernel_{wl_name}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)), "measured"
+    return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def run_ours(args, wl, rank, world, dist):
+    import ctypes
+
+    import torch
+
+    from indexgen_b200 import Context, build_conflict_graph
+    from indexgen_b200._lib import check, lib
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    words, L, d = wl["words"], wl["L"], wl["min_ed"]
+    n = len(words)
+    pairs = pairs_of(n)
+    ctx = Context(dev)
+    ext = torch.cuda.ExternalStream(ctx.stream)
+    words_dev = torch.from_numpy(words.view(np.int32)).to(f"cuda:{dev}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    torch.cuda.synchronize()
+
+    edges = None
+    for _ in range(args.warmup):
+        with build_conflict_graph(words_dev, L, d, ctx) as G:
+            edges = G.edges
+    props = torch.cuda.get_device_properties(dev)
+    bus = None
+    for attr in ("pci_bus_id",):
+        if hasattr(props, attr) and hasattr(props, "pci_domain_id") and hasattr(props, "pci_device_id"):
+            bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}"
+
+    # ---- device-resident timing
+    ctx.set_profiling(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(bus)
+    clocks.start()
+    launches0 = ctx.launches
+    step_ms = []
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (256 MiB > 126 MB L2), untimed
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        G = build_conflict_graph(words_dev, L, d, ctx)
+        e1.record(ext)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        G.close()
+    torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    pair_ms, pair_launches = ctx.phase_time(0)
+    comp_ms, comp_launches = ctx.phase_time(1)
+    ctx.set_profiling(False)
+    if dist:
+        t = torch.tensor([total_ms], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * pairs * args.steps / (total_ms / 1e3) / 1e9
+
+    # ---- end to end through the public API with pinned host buffers
+    h_words = torch.from_numpy(words.view(np.int32)).pin_memory()
+    h_row = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    h_cols = torch.empty(max(edges, 1), dtype=torch.int32, pin_memory=True)
+    e2e_steps = max(3, min(args.steps, 10))
+    wall = []
+    for _ in range(e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        h = ctypes.c_void_p()
+        check(lib().ig_graph_build(ctx.handle, ctypes.c_void_p(h_words.data_ptr()), n, L, d, 0, ctypes.byref(h)),
+              "ig_graph_build", ctx.handle)
+        check(lib().ig_graph_upper_csr(h, ctypes.c_void_p(h_row.data_ptr()), ctypes.c_void_p(h_cols.data_ptr())),
+              "ig_graph_upper_csr", ctx.handle)
+        t1 = time.perf_counter()
+        lib().ig_graph_free(h)
+        wall.append(t1 - t0)
+    e2e_s = sum(wall) / len(wall)
+    if dist:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 4 * n,
+           "d2h_bytes_per_step": 8 * (n + 1) + 4 * edges, "ms_per_step": 1e3 * e2e_s,
+           "note": "ig_graph_build(host words) + ig_graph_upper_csr(host buffers), wall clock"}
+
+    # ---- greedy codebook (sequential, host) on the same graph, reported apart
+    with build_conflict_graph(words_dev, L, d, ctx) as G:
+        t0 = time.perf_counter()
+        sel = G.codebook(1)
+        greedy_ms = 1e3 * (time.perf_counter() - t0)
+
+    peaks, src = measured_peaks()
+    sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    int32_peak = props.multi_processor_count * 128 * sm_mhz * 1e6 / 1e12
+    ops = pairs * 16 * L
+    pair_avg_s = (pair_ms / max(pair_launches, 1)) / 1e3
+    achieved = ops / pair_avg_s / 1e12 if pair_launches else None
+    traffic = profile_traffic(wl["name"])
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    # compaction lower bound: edge records read (16 B) + columns written (4 B)
+    # + row offsets written and scanned in place (3 x 8 B per row)
+    comp_bytes = 16 * edges + 4 * edges + 24 * (n + 1)
+    comp_avg_s = (comp_ms / max(comp_launches, 1)) / 1e3
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(step_ms), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": wl["name"], "desc": wl["desc"], "n": n, "L": L, "min_ed": d,
+                   "pairs_per_step": pairs, "edges": edges, "parallelism": f"replicas x{world}",
+                   "l2": "flushed between steps (256 MiB device write, untimed)"},
+        "e2e": e2e,
+        "roofline": {"bound": "int32-issue", "achieved": achieved, "peak": int32_peak, "unit": "Tops/s",
+                     "frac": (achieved / int32_peak) if achieved else None, "traffic": traffic,
+                     "kernel": "pair_kernel", "kernel_ms_per_launch": pair_avg_s * 1e3,
+                     "work": f"{pairs} pair tests x 16*L={16 * L} int ops per launch",
+                     "peak_source": f"{props.multi_processor_count} SMs x 128 INT32 lanes x {sm_mhz:.0f} MHz "
+                                    f"max SM clock ({src} MEASURED_PEAKS sm_max_mhz)"},
+        "compaction": {"bound": "hbm", "achieved": comp_bytes / comp_avg_s / 1e9 if comp_launches else None,
+                       "peak": hbm_peak, "unit": "GB/s",
+                       "frac": (comp_bytes / comp_avg_s / 1e9 / hbm_peak) if comp_launches else None,
+                       "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "greedy": {"ms": greedy_ms, "codebook": int(len(sel)), "order_threads": 1, "where": "host C++ (library)"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(wl)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    wl = workload(args.workload)
+    if args.impl == "reference":
+        run_reference(args, wl, rank)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        run_ours(args, wl, rank, world, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,130 @@
+/* libindexgen_cuda -- B200 (sm_100a) conflict-graph + greedy codebook library.
+ *
+ * C ABI that replaces the reference's GPU boundary: the C++ host of IndexGen
+ * calls these entry points where it shells out to
+ *     python3 src/gpu_graph_generator.py <cands.txt> <edges.bin> <minED> <maxGB>
+ * (src/SparseMat.cpp:454-534, FillAdjListGPU) and where it runs the
+ * independent-set solve (src/SparseMat.cpp:679-851).  Plain pointers and sizes
+ * only; no exceptions cross this boundary; every call returns an ig_status.
+ *
+ * Words: one uint32 per candidate of length len (1..16) over {0,1,2,3}
+ * (A=0, C=1, G=2, T=3); character p is stored in bits 2p..2p+1.  Bits above
+ * 2*len are ignored.
+ *
+ * Edge predicate: i<j is an edge iff Levenshtein(c_i, c_j) < min_ed, the
+ * negation of EditDistanceBandedAtLeast(c_j, MakePattern(c_i), min_ed)
+ * (include/EditDistance.hpp:368-372) used by FillAdjListTH
+ * (src/SparseMat.cpp:536-565) and of `score < threshold` in
+ * src/cuda_edit_distance.py:195.
+ */
+#ifndef INDEXGEN_CUDA_H
+#define INDEXGEN_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IG_MAX_LEN 16
+
+typedef enum ig_status {
+    IG_OK = 0,
+    IG_ERR_INPUT = 1,     /* bad argument: length, symbol, size, null pointer   */
+    IG_ERR_CAPACITY = 2,  /* a caller buffer or a fixed limit is too small       */
+    IG_ERR_OOM = 3,       /* device or host allocation failed / over budget     */
+    IG_ERR_CUDA = 4,      /* a CUDA runtime call failed                         */
+    IG_ERR_TIMEOUT = 5,   /* a bounded device wait gave up                      */
+    IG_ERR_CANCELLED = 6, /* a queued job was cancelled                         */
+    IG_ERR_STATE = 7      /* call made on an object in the wrong state          */
+} ig_status;
+
+typedef struct ig_ctx ig_ctx;     /* device, stream and reusable workspace       */
+typedef struct ig_graph ig_graph; /* one conflict graph, CSR resident in HBM     */
+
+/* ---- library / context ------------------------------------------------- */
+
+const char *ig_version(void);
+const char *ig_status_string(ig_status s);
+
+/* Creates a context on `device`.  A context owns one CUDA stream and a
+ * workspace that grows to the largest job seen; calls on one context are
+ * serialised internally (safe to share between host threads). */
+ig_status ig_ctx_create(ig_ctx **out, int device);
+ig_status ig_ctx_destroy(ig_ctx *ctx);
+/* Message of the last failure on this context (thread-unsafe snapshot). */
+const char *ig_last_error(const ig_ctx *ctx);
+/* The context's cudaStream_t, for callers that time or order device work. */
+ig_status ig_ctx_stream(ig_ctx *ctx, void **stream);
+/* Pre-size the edge workspace (optional; it otherwise grows on demand). */
+ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges);
+/* Number of device kernels this context has launched so far. */
+int64_t ig_ctx_launches(const ig_ctx *ctx);
+/* Per-phase device timing with CUDA events on the context's stream (off by
+ * default).  Phases: IG_PHASE_PAIRS (the pair-test kernel), IG_PHASE_COMPACT
+ * (row prefix + scan + scatter into CSR), IG_PHASE_PREP (selector streams).
+ * ig_ctx_phase_time returns the accumulated milliseconds and launch count
+ * since profiling was last enabled. */
+#define IG_PHASE_PAIRS 0
+#define IG_PHASE_COMPACT 1
+#define IG_PHASE_PREP 2
+ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable);
+ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches);
+
+/* ---- host-side input preparation (no device work) ---------------------- */
+
+/* '0'..'3' text rows, `stride` bytes apart, to packed words.  Replaces the
+ * text load + pack of src/gpu_graph_generator.py:11-15 and
+ * src/cuda_edit_distance.py:246-255.  On a bad symbol returns IG_ERR_INPUT and
+ * stores the failing row in *bad_row (if non-null). */
+ig_status ig_pack(const char *text, int64_t n, int len, int64_t stride, uint32_t *out, int64_t *bad_row);
+
+/* Homopolymer-run and GC-content filters of CandidateGenerator::applyFilters
+ * (src/CandidateGenerator.cpp:24-50; MaxRun / TestGCCont, src/Utils.cpp:420-462,
+ * same double comparisons).  keep[i] = 1 when word i passes. */
+ig_status ig_filter(const uint32_t *words, int64_t n, int len, int max_run, double min_gc, double max_gc,
+                    uint8_t *keep);
+
+/* ---- conflict graph (FillAdjListGPU, src/SparseMat.cpp:454-534) -------- */
+
+/* Builds the graph of all pairs i<j with ED < min_ed.  `words` is a host
+ * pointer, or a device pointer when words_on_device != 0 (it must then be
+ * ready on the context's stream).  The result stays in HBM as an upper CSR
+ * with ascending columns.  Blocks until the graph is complete. */
+ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
+                         ig_graph **out);
+ig_status ig_graph_free(ig_graph *g);
+/* n and the number of edges (u<v); matrixOnesNum of the reference = 2*edges. */
+ig_status ig_graph_stats(const ig_graph *g, int32_t *n, int64_t *edges);
+/* Upper CSR to host buffers: row_ptr[n+1], cols[edges] (ascending per row). */
+ig_status ig_graph_upper_csr(const ig_graph *g, int64_t *row_ptr, int32_t *cols);
+/* Edges as int32 (u, v) pairs, u<v, rows ascending, columns ascending: the
+ * binary edge-file layout that AdjList::FromBinaryFile reads
+ * (src/gpu_graph_generator.py:49-77, src/SparseMat.cpp:338-390). */
+ig_status ig_graph_pairs(const ig_graph *g, int32_t *pairs);
+/* Device pointers of the resident upper CSR (valid until ig_graph_free). */
+ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const int32_t **cols);
+/* Greedy minimum-degree independent set over the graph, reproducing AdjList's
+ * selection order (src/SparseMat.cpp:81-266, :679-731) for neighbour lists
+ * assembled as FillAdjList(order_threads) does (src/SparseMat.cpp:599-609);
+ * order_threads = 1 is the sorted order the GPU-path loader builds.
+ * order[] receives up to n vertex ids in selection order; *count their number. */
+ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int32_t *count);
+
+/* ---- one-call conveniences --------------------------------------------- */
+
+/* SolveIndependentSet (src/SparseMat.cpp:784-851): graph + greedy.
+ * edges may be null. */
+ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,
+                   int32_t *order, int32_t *count, int64_t *edges);
+/* Number of conflicting pairs only (VerifyDist's GPU branch passes when it is
+ * zero, src/Utils.cpp:203-288). */
+ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *edges);
+/* Greedy over a caller-supplied upper CSR in host memory (no device work). */
+ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
+                                     int32_t *order, int32_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INDEXGEN_CUDA_H */

@@ -1,0 +1,25 @@
+"""indexgen_b200 -- B200-native conflict-graph + greedy codebook path of IndexGen.
+
+The compute lives in libindexgen_cuda.so (hand-written CUDA for sm_100a behind
+the C ABI of include/indexgen_cuda.h); this package is the Python host mirror
+of the reference's GPU path (src/cuda_edit_distance.py, src/gpu_graph_generator.py,
+SolveIndependentSet / VerifyDist of src/SparseMat.cpp, src/Utils.cpp).
+"""
+from .graph import (  # noqa: F401
+    ConflictGraph,
+    Context,
+    IndexGenError,
+    apply_filters,
+    build_conflict_graph,
+    codebook_from_upper_csr,
+    count_conflicts,
+    default_context,
+    fill_adj_list_gpu,
+    pack_sequences,
+    solve,
+    solve_edit_distance_cuda,
+    solve_independent_set,
+    verify_dist,
+)
+
+__version__ = "0.1.0"

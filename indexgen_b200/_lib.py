@@ -1,0 +1,96 @@
+"""ctypes binding of libindexgen_cuda.so (the C ABI in include/indexgen_cuda.h).
+
+The shared object is built in-tree by ``indexgen_b200.build``.  Loading fails
+loudly when it is missing: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libindexgen_cuda.so")
+
+# Every entry point include/indexgen_cuda.h declares.
+EXPORTS = (
+    "ig_version", "ig_status_string", "ig_ctx_create", "ig_ctx_destroy", "ig_last_error", "ig_ctx_stream",
+    "ig_ctx_reserve", "ig_ctx_launches", "ig_ctx_set_profiling", "ig_ctx_phase_time", "ig_pack", "ig_filter", "ig_graph_build", "ig_graph_free",
+    "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_codebook",
+    "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr",
+)
+
+STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
+          5: "IG_ERR_TIMEOUT", 6: "IG_ERR_CANCELLED", 7: "IG_ERR_STATE"}
+
+
+class IndexGenError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str = ""):
+        self.status = status
+        self.code = STATUS.get(status, str(status))
+        super().__init__(f"{where}: {self.code}" + (f" ({detail})" if detail else ""))
+
+
+_lib = None
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_int = ctypes.c_int
+
+
+def _declare(L):
+    sig = {
+        "ig_version": (ctypes.c_char_p, []),
+        "ig_status_string": (ctypes.c_char_p, [_int]),
+        "ig_ctx_create": (_int, [ctypes.POINTER(_vp), _int]),
+        "ig_ctx_destroy": (_int, [_vp]),
+        "ig_last_error": (ctypes.c_char_p, [_vp]),
+        "ig_ctx_stream": (_int, [_vp, ctypes.POINTER(_vp)]),
+        "ig_ctx_reserve": (_int, [_vp, _i64]),
+        "ig_ctx_launches": (_i64, [_vp]),
+        "ig_ctx_set_profiling": (_int, [_vp, _int]),
+        "ig_ctx_phase_time": (_int, [_vp, _int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_i64)]),
+        "ig_pack": (_int, [ctypes.c_char_p, _i64, _int, _i64, _vp, ctypes.POINTER(_i64)]),
+        "ig_filter": (_int, [_vp, _i64, _int, _int, ctypes.c_double, ctypes.c_double, _vp]),
+        "ig_graph_build": (_int, [_vp, _vp, _i32, _int, _int, _int, ctypes.POINTER(_vp)]),
+        "ig_graph_free": (_int, [_vp]),
+        "ig_graph_stats": (_int, [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
+        "ig_graph_upper_csr": (_int, [_vp, _vp, _vp]),
+        "ig_graph_pairs": (_int, [_vp, _vp]),
+        "ig_graph_device_csr": (_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+        "ig_graph_codebook": (_int, [_vp, _int, _vp, ctypes.POINTER(_i32)]),
+        "ig_solve": (_int, [_vp, _vp, _i32, _int, _int, _int, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
+        "ig_count_conflicts": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),
+        "ig_codebook_from_upper_csr": (_int, [_vp, _vp, _i32, _int, _vp, ctypes.POINTER(_i32)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+
+
+def lib():
+    """Load libindexgen_cuda.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m indexgen_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def check(status: int, where: str, ctx=None):
+    if status != 0:
+        detail = ""
+        if ctx:
+            msg = lib().ig_last_error(ctx)
+            detail = msg.decode() if msg else ""
+        raise IndexGenError(status, where, detail)
+
+
+def ptr(a: np.ndarray) -> int:
+    return a.ctypes.data if a.size else 0

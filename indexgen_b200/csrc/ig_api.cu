@@ -1,0 +1,410 @@
+// C ABI of libindexgen_cuda (declarations and reference citations in
+// include/indexgen_cuda.h).
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "ig_internal.h"
+
+struct ig_ctx : ig::Ctx {
+};
+struct ig_graph : ig::Graph {
+};
+
+namespace ig {
+
+ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg)
+{
+    if (ctx)
+        ctx->last_error = msg;
+    return s;
+}
+
+ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what)
+{
+    cudaGetLastError();
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? IG_ERR_OOM : IG_ERR_CUDA,
+                     std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+// Makes ctx->device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
+
+ig_status check_job(const uint32_t *words, int32_t n, int len)
+{
+    if (n < 0 || len < 1 || len > IG_MAX_LEN || (n > 0 && !words))
+        return IG_ERR_INPUT;
+    return IG_OK;
+}
+
+// Device copy of the words (host input) or the caller's device pointer.
+ig_status stage_words(Ctx *ctx, const uint32_t *words, int32_t n, int on_device, const uint32_t **d_words)
+{
+    if (on_device || n == 0) {
+        *d_words = words;
+        return IG_OK;
+    }
+    const size_t bytes = (size_t)n * sizeof(uint32_t);
+    if (ctx->words.bytes < bytes) {
+        if (ctx->words.ptr)
+            cudaFreeAsync(ctx->words.ptr, ctx->stream);
+        ctx->words.ptr = nullptr;
+        ctx->words.bytes = 0;
+        cudaError_t e = cudaMallocAsync(&ctx->words.ptr, bytes, ctx->stream);
+        if (e != cudaSuccess)
+            return cuda_error(ctx, e, "word buffer allocation");
+        ctx->words.bytes = bytes;
+    }
+    cudaError_t e = cudaMemcpyAsync(ctx->words.ptr, words, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, "word upload");
+    *d_words = static_cast<const uint32_t *>(ctx->words.ptr);
+    return IG_OK;
+}
+
+void release_graph(ig_graph *g)
+{
+    if (!g)
+        return;
+    if (g->ctx) {
+        DeviceGuard dg(g->ctx->device);
+        if (g->d_row_ptr)
+            cudaFreeAsync(g->d_row_ptr, g->ctx->stream);
+        if (g->d_cols)
+            cudaFreeAsync(g->d_cols, g->ctx->stream);
+        cudaStreamSynchronize(g->ctx->stream);
+    }
+    delete g;
+}
+
+ig_status fetch_host(ig_graph *g)
+{
+    if (g->host_valid)
+        return IG_OK;
+    Ctx *ctx = g->ctx;
+    DeviceGuard dg(ctx->device);
+    try {
+        g->h_row_ptr.resize((size_t)g->n + 1);
+        g->h_cols.resize((size_t)std::max<int64_t>(g->edges, 1));
+    } catch (...) {
+        return set_error(ctx, IG_ERR_OOM, "host CSR allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(g->h_row_ptr.data(), g->d_row_ptr, ((size_t)g->n + 1) * sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && g->edges > 0)
+        e = cudaMemcpyAsync(g->h_cols.data(), g->d_cols, (size_t)g->edges * sizeof(int32_t),
+                            cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, "CSR download");
+    g->host_valid = true;
+    return IG_OK;
+}
+
+}  // namespace
+}  // namespace ig
+
+extern "C" {
+
+const char *ig_version(void) { return "indexgen_b200 0.1 (sm_100a)"; }
+
+const char *ig_status_string(ig_status s)
+{
+    switch (s) {
+    case IG_OK: return "ok";
+    case IG_ERR_INPUT: return "invalid input";
+    case IG_ERR_CAPACITY: return "capacity exceeded";
+    case IG_ERR_OOM: return "out of memory";
+    case IG_ERR_CUDA: return "CUDA error";
+    case IG_ERR_TIMEOUT: return "device wait timed out";
+    case IG_ERR_CANCELLED: return "cancelled";
+    case IG_ERR_STATE: return "invalid state";
+    }
+    return "unknown status";
+}
+
+ig_status ig_ctx_create(ig_ctx **out, int device)
+{
+    if (!out)
+        return IG_ERR_INPUT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return device < 0 ? IG_ERR_INPUT : IG_ERR_CUDA;
+    }
+    ig_ctx *c = new (std::nothrow) ig_ctx();
+    if (!c)
+        return IG_ERR_OOM;
+    c->device = device;
+    ig::DeviceGuard dg(device);
+    cudaDeviceProp prop;
+    if (!dg.ok || cudaGetDeviceProperties(&prop, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return IG_ERR_CUDA;
+    }
+    c->sm_count = prop.multiProcessorCount;
+    // Keep freed stream-ordered allocations cached in the device pool so that
+    // repeated jobs do not go back to the driver.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    cudaGetLastError();
+    *out = c;
+    return IG_OK;
+}
+
+ig_status ig_ctx_destroy(ig_ctx *ctx)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    {
+        ig::DeviceGuard dg(ctx->device);
+        for (ig::DevBuf *b : {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags})
+            if (b->ptr)
+                cudaFreeAsync(b->ptr, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        cudaStreamDestroy(ctx->stream);
+        for (cudaEvent_t e : ctx->ev)
+            if (e)
+                cudaEventDestroy(e);
+        cudaGetLastError();
+    }
+    delete ctx;
+    return IG_OK;
+}
+
+const char *ig_last_error(const ig_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+ig_status ig_ctx_stream(ig_ctx *ctx, void **stream)
+{
+    if (!ctx || !stream)
+        return IG_ERR_INPUT;
+    *stream = (void *)ctx->stream;
+    return IG_OK;
+}
+
+int64_t ig_ctx_launches(const ig_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (enable && !ctx->ev[0]) {
+        for (cudaEvent_t &e : ctx->ev)
+            if (cudaEventCreate(&e) != cudaSuccess)
+                return ig::cuda_error(ctx, cudaGetLastError(), "cudaEventCreate");
+    }
+    ctx->profiling = enable != 0;
+    for (int p = 0; p < 3; ++p) {
+        ctx->phase_ms[p] = 0;
+        ctx->phase_launches[p] = 0;
+        ctx->phase_pending[p] = false;
+    }
+    return IG_OK;
+}
+
+ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches)
+{
+    if (!ctx || phase < 0 || phase > 2)
+        return IG_ERR_INPUT;
+    if (ms)
+        *ms = ctx->phase_ms[phase];
+    if (launches)
+        *launches = ctx->phase_launches[phase];
+    return IG_OK;
+}
+
+ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges)
+{
+    if (!ctx || edges < 0)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if ((unsigned long long)edges <= ctx->rec_capacity)
+        return IG_OK;
+    if (ctx->records.ptr)
+        cudaFreeAsync(ctx->records.ptr, ctx->stream);
+    ctx->records.ptr = nullptr;
+    ctx->records.bytes = 0;
+    ctx->rec_capacity = 0;
+    const size_t bytes = (size_t)edges * sizeof(ig::EdgeRecord);
+    cudaError_t e = cudaMallocAsync(&ctx->records.ptr, bytes, ctx->stream);
+    if (e != cudaSuccess)
+        return ig::cuda_error(ctx, e, "edge record reservation");
+    ctx->records.bytes = bytes;
+    ctx->rec_capacity = (unsigned long long)edges;
+    return IG_OK;
+}
+
+ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
+                         ig_graph **out)
+{
+    if (!ctx || !out)
+        return IG_ERR_INPUT;
+    *out = nullptr;
+    if (ig::check_job(words, n, len) != IG_OK)
+        return ig::set_error(ctx, IG_ERR_INPUT, "words must be non-null, n >= 0 and 1 <= len <= 16");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    ig_graph *g = new (std::nothrow) ig_graph();
+    if (!g)
+        return IG_ERR_OOM;
+    const uint32_t *d_words = nullptr;
+    ig_status s = ig::stage_words(ctx, words, n, words_on_device, &d_words);
+    if (s == IG_OK)
+        s = ig::build_graph(ctx, d_words, n, len, min_ed, g);
+    if (s != IG_OK) {
+        ig::release_graph(g);
+        return s;
+    }
+    *out = g;
+    return IG_OK;
+}
+
+ig_status ig_graph_free(ig_graph *g)
+{
+    if (!g)
+        return IG_ERR_INPUT;
+    ig::release_graph(g);
+    return IG_OK;
+}
+
+ig_status ig_graph_stats(const ig_graph *g, int32_t *n, int64_t *edges)
+{
+    if (!g)
+        return IG_ERR_INPUT;
+    if (n)
+        *n = g->n;
+    if (edges)
+        *edges = g->edges;
+    return IG_OK;
+}
+
+ig_status ig_graph_upper_csr(const ig_graph *g, int64_t *row_ptr, int32_t *cols)
+{
+    if (!g || !row_ptr || (g->edges > 0 && !cols))
+        return IG_ERR_INPUT;
+    ig::Ctx *ctx = g->ctx;
+    if (g->host_valid) {
+        std::memcpy(row_ptr, g->h_row_ptr.data(), ((size_t)g->n + 1) * sizeof(int64_t));
+        if (g->edges > 0)
+            std::memcpy(cols, g->h_cols.data(), (size_t)g->edges * sizeof(int32_t));
+        return IG_OK;
+    }
+    // straight from HBM into the caller's buffers (a DMA when they are pinned)
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    cudaError_t e = cudaMemcpyAsync(row_ptr, g->d_row_ptr, ((size_t)g->n + 1) * sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && g->edges > 0)
+        e = cudaMemcpyAsync(cols, g->d_cols, (size_t)g->edges * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return ig::cuda_error(ctx, e, "CSR download");
+    return IG_OK;
+}
+
+ig_status ig_graph_pairs(const ig_graph *gc, int32_t *pairs)
+{
+    ig_graph *g = const_cast<ig_graph *>(gc);
+    if (!g || (g->edges > 0 && !pairs))
+        return IG_ERR_INPUT;
+    ig_status s = ig::fetch_host(g);
+    if (s != IG_OK)
+        return s;
+    int64_t k = 0;
+    for (int32_t r = 0; r < g->n; ++r)
+        for (int64_t e = g->h_row_ptr[(size_t)r]; e < g->h_row_ptr[(size_t)r + 1]; ++e) {
+            pairs[2 * k] = r;
+            pairs[2 * k + 1] = g->h_cols[(size_t)e];
+            ++k;
+        }
+    return IG_OK;
+}
+
+ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const int32_t **cols)
+{
+    if (!g || !row_ptr || !cols)
+        return IG_ERR_INPUT;
+    *row_ptr = g->d_row_ptr;
+    *cols = g->d_cols;
+    return IG_OK;
+}
+
+ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int32_t *count)
+{
+    if (!g || !count || order_threads < 1 || (g->n > 0 && !order))
+        return IG_ERR_INPUT;
+    ig_status s = ig::fetch_host(g);
+    if (s != IG_OK)
+        return s;
+    try {
+        *count = ig::greedy_from_upper(g->h_row_ptr.data(), g->h_cols.data(), g->n, order_threads, order);
+    } catch (...) {
+        return ig::set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
+    }
+    return IG_OK;
+}
+
+ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,
+                   int32_t *order, int32_t *count, int64_t *edges)
+{
+    if (!ctx || !count || order_threads < 1 || (n > 0 && !order))
+        return IG_ERR_INPUT;
+    ig_graph *g = nullptr;
+    ig_status s = ig_graph_build(ctx, words, n, len, min_ed, 0, &g);
+    if (s != IG_OK)
+        return s;
+    if (edges)
+        *edges = g->edges;
+    s = ig_graph_codebook(g, order_threads, order, count);
+    ig::release_graph(g);
+    return s;
+}
+
+ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *edges)
+{
+    if (!ctx || !edges)
+        return IG_ERR_INPUT;
+    if (ig::check_job(words, n, len) != IG_OK)
+        return ig::set_error(ctx, IG_ERR_INPUT, "words must be non-null, n >= 0 and 1 <= len <= 16");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    const uint32_t *d_words = nullptr;
+    ig_status s = ig::stage_words(ctx, words, n, 0, &d_words);
+    if (s != IG_OK)
+        return s;
+    return ig::count_edges(ctx, d_words, n, len, min_ed, edges);
+}
+
+}  // extern "C"

@@ -1,0 +1,91 @@
+// Internal declarations shared by the libindexgen_cuda translation units.
+#pragma once
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "indexgen_cuda.h"
+
+namespace ig {
+
+// Rows of one band = threads of one pair-test CTA; columns of one staged tile.
+constexpr int kBandRows = 256;
+constexpr int kTileCols = 256;
+
+// One emitted edge: (row, col, rank of col inside (row, segment), segment).
+// Ranks make the CSR scatter order-exact without a sort.
+struct EdgeRecord {
+    uint32_t row, col, rank, seg;
+};
+
+// Grow-only device buffer owned by a context.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string last_error;
+    int64_t launches = 0;
+    // workspace
+    DevBuf words, sel, counts, records, scan_tmp, flags;
+    unsigned long long rec_capacity = 0;  // records that fit in `records`
+    // optional per-phase timing (IG_PHASE_*)
+    bool profiling = false;
+    cudaEvent_t ev[6] = {};
+    double phase_ms[3] = {0, 0, 0};
+    int64_t phase_launches[3] = {0, 0, 0};
+    bool phase_pending[3] = {false, false, false};
+};
+
+// Records an event pair around a phase when profiling is on.
+void phase_begin(Ctx *ctx, int phase);
+void phase_end(Ctx *ctx, int phase);
+void phase_collect(Ctx *ctx);  // after a stream sync: fold finished pairs in
+
+struct Graph {
+    Ctx *ctx = nullptr;
+    int32_t n = 0;
+    int len = 0;
+    int min_ed = 0;
+    int64_t edges = 0;
+    int64_t *d_row_ptr = nullptr;  // [n+1]
+    int32_t *d_cols = nullptr;     // [edges]
+    // host copies, filled on first use
+    std::vector<int64_t> h_row_ptr;
+    std::vector<int32_t> h_cols;
+    bool host_valid = false;
+};
+
+// Geometry of the upper-triangle work decomposition for one job.
+struct PairPlan {
+    int32_t n = 0;
+    int seg_shift = 0;     // segment width = 1 << seg_shift columns (multiple of kBandRows)
+    int nseg = 0;          // segments covering [0, n)
+    int bands_per_seg = 0; // segment width / kBandRows
+    int nbands = 0;
+    long long items = 0;   // (band, segment) work items in the upper triangle
+};
+
+PairPlan make_plan(int32_t n, int grid_ctas);
+
+// Device pipeline stages (ig_graph.cu).
+ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, Graph *g);
+ig_status count_edges(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, int64_t *edges);
+
+// Host greedy (ig_host.cpp).
+int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
+                          int32_t *order);
+
+ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
+ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);
+
+}  // namespace ig

@@ -1,0 +1,296 @@
+"""Python host API over libindexgen_cuda, mirroring the reference's GPU path.
+
+Reference interface this mirrors (same names, argument meaning, errors):
+
+* ``pack_sequences(strings)``                 src/cuda_edit_distance.py:246-255
+* ``solve_edit_distance_cuda(strings, threshold, tile_size, max_gpu_memory_gb)``
+                                              src/cuda_edit_distance.py:278-446
+  returns the adjacency lists (both directions; here in ascending order).
+* ``fill_adj_list_gpu(candidates, min_ed, ...)`` FillAdjListGPU, src/SparseMat.cpp:454-534:
+  the conflict graph and matrixOnesNum (= 2 * edges).
+* ``solve_independent_set(candidates, min_ed, thread_num)``
+                                              SolveIndependentSet, src/SparseMat.cpp:784-851
+* ``verify_dist(codebook, min_ed)``          VerifyDist GPU branch, src/Utils.cpp:203-288
+* ``apply_filters(words, L, ...)``           CandidateGenerator::applyFilters, src/CandidateGenerator.cpp:24-50
+
+All device work goes through the C ABI; nothing here computes a distance.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import IndexGenError, check, lib, ptr
+
+
+class Context:
+    """One device, one CUDA stream, a reusable HBM workspace (ig_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().ig_ctx_create(ctypes.byref(h), int(device)), "ig_ctx_create")
+        self.handle = h
+        self.device = int(device)
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        check(lib().ig_ctx_stream(self.handle, ctypes.byref(s)), "ig_ctx_stream", self.handle)
+        return int(s.value or 0)
+
+    @property
+    def launches(self) -> int:
+        return int(lib().ig_ctx_launches(self.handle))
+
+    def set_profiling(self, enable: bool):
+        check(lib().ig_ctx_set_profiling(self.handle, int(bool(enable))), "ig_ctx_set_profiling", self.handle)
+
+    def phase_time(self, phase: int):
+        """(milliseconds, launches) accumulated for IG_PHASE_{PAIRS=0, COMPACT=1, PREP=2}."""
+        ms = ctypes.c_double()
+        n = ctypes.c_int64()
+        check(lib().ig_ctx_phase_time(self.handle, int(phase), ctypes.byref(ms), ctypes.byref(n)),
+              "ig_ctx_phase_time", self.handle)
+        return float(ms.value), int(n.value)
+
+    def reserve(self, edges: int):
+        check(lib().ig_ctx_reserve(self.handle, int(edges)), "ig_ctx_reserve", self.handle)
+
+    def close(self):
+        if self.handle:
+            lib().ig_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default
+    with _default_lock:
+        if _default is None:
+            _default = Context(0)
+        return _default
+
+
+def _words_array(words) -> np.ndarray:
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    if w.ndim != 1:
+        raise ValueError("words must be a 1-D array of packed uint32")
+    return w
+
+
+class ConflictGraph:
+    """A conflict graph resident in HBM as an upper CSR (ig_graph)."""
+
+    def __init__(self, handle, ctx: Context, L: int, min_ed: int):
+        self.handle = handle
+        self.ctx = ctx
+        self.L = L
+        self.min_ed = min_ed
+        n = ctypes.c_int32()
+        e = ctypes.c_int64()
+        check(lib().ig_graph_stats(handle, ctypes.byref(n), ctypes.byref(e)), "ig_graph_stats")
+        self.n = int(n.value)
+        self.edges = int(e.value)
+
+    @property
+    def matrix_ones_num(self) -> int:
+        """The reference's 'Number of Ones in Matrix' (both directions)."""
+        return 2 * self.edges
+
+    def upper_csr(self):
+        row_ptr = np.zeros(self.n + 1, np.int64)
+        cols = np.zeros(self.edges, np.int32)
+        check(lib().ig_graph_upper_csr(self.handle, ptr(row_ptr), ptr(cols)), "ig_graph_upper_csr",
+              self.ctx.handle)
+        return row_ptr, cols
+
+    def pairs(self) -> np.ndarray:
+        """(u, v) int32 pairs, u < v: the reference's binary edge-file layout."""
+        out = np.zeros((self.edges, 2), np.int32)
+        check(lib().ig_graph_pairs(self.handle, ptr(out)), "ig_graph_pairs", self.ctx.handle)
+        return out
+
+    def device_csr(self):
+        rp = ctypes.c_void_p()
+        cl = ctypes.c_void_p()
+        check(lib().ig_graph_device_csr(self.handle, ctypes.byref(rp), ctypes.byref(cl)), "ig_graph_device_csr")
+        return int(rp.value or 0), int(cl.value or 0)
+
+    def codebook(self, order_threads: int = 1) -> np.ndarray:
+        order = np.zeros(max(self.n, 1), np.int32)
+        cnt = ctypes.c_int32()
+        check(lib().ig_graph_codebook(self.handle, int(order_threads), ptr(order), ctypes.byref(cnt)),
+              "ig_graph_codebook", self.ctx.handle)
+        return order[: cnt.value]
+
+    def adj_list(self):
+        """Neighbour lists in both directions, ascending (list of lists)."""
+        row_ptr, cols = self.upper_csr()
+        adj = [[] for _ in range(self.n)]
+        rows = np.repeat(np.arange(self.n), np.diff(row_ptr))
+        for u, v in zip(rows.tolist(), cols.tolist()):
+            adj[v].append(u)
+        for u in range(self.n):
+            adj[u].extend(cols[row_ptr[u]:row_ptr[u + 1]].tolist())
+        return adj
+
+    def close(self):
+        if self.handle:
+            lib().ig_graph_free(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_conflict_graph(words, L: int, min_ed: int, ctx: Context | None = None) -> ConflictGraph:
+    """Conflict graph of packed words (numpy uint32, or a CUDA tensor/array
+    exposing ``data_ptr()`` whose data is already on the context's device)."""
+    ctx = ctx or default_context()
+    h = ctypes.c_void_p()
+    if hasattr(words, "data_ptr") and getattr(words, "is_cuda", False):
+        n = int(words.numel())
+        check(lib().ig_graph_build(ctx.handle, ctypes.c_void_p(words.data_ptr()), n, int(L), int(min_ed), 1,
+                                   ctypes.byref(h)), "ig_graph_build", ctx.handle)
+    else:
+        w = _words_array(words)
+        check(lib().ig_graph_build(ctx.handle, ptr(w), len(w), int(L), int(min_ed), 0, ctypes.byref(h)),
+              "ig_graph_build", ctx.handle)
+    return ConflictGraph(h, ctx, int(L), int(min_ed))
+
+
+def count_conflicts(words, L: int, min_ed: int, ctx: Context | None = None) -> int:
+    ctx = ctx or default_context()
+    w = _words_array(words)
+    e = ctypes.c_int64()
+    check(lib().ig_count_conflicts(ctx.handle, ptr(w), len(w), int(L), int(min_ed), ctypes.byref(e)),
+          "ig_count_conflicts", ctx.handle)
+    return int(e.value)
+
+
+def codebook_from_upper_csr(row_ptr, cols, n: int, order_threads: int = 1) -> np.ndarray:
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    cl = np.ascontiguousarray(cols, dtype=np.int32)
+    order = np.zeros(max(n, 1), np.int32)
+    cnt = ctypes.c_int32()
+    check(lib().ig_codebook_from_upper_csr(ptr(rp), ptr(cl), int(n), int(order_threads), ptr(order),
+                                           ctypes.byref(cnt)), "ig_codebook_from_upper_csr")
+    return order[: cnt.value]
+
+
+def solve(words, L: int, min_ed: int, order_threads: int = 1, ctx: Context | None = None):
+    """Graph + greedy in one call: (selected ids in order, edges)."""
+    ctx = ctx or default_context()
+    w = _words_array(words)
+    order = np.zeros(max(len(w), 1), np.int32)
+    cnt = ctypes.c_int32()
+    e = ctypes.c_int64()
+    check(lib().ig_solve(ctx.handle, ptr(w), len(w), int(L), int(min_ed), int(order_threads), ptr(order),
+                         ctypes.byref(cnt), ctypes.byref(e)), "ig_solve", ctx.handle)
+    return order[: cnt.value], int(e.value)
+
+
+# ---------------------------------------------------------------------------
+# Reference-named entry points
+# ---------------------------------------------------------------------------
+
+def pack_sequences(strings):
+    """Strings over '0'..'3' -> (packed words, L, N).  Mirrors
+    src/cuda_edit_distance.py:246-255 (which returns flat uint8 symbols); the
+    words here hold 2 bits per symbol.  Raises ValueError on a bad symbol or
+    ragged lengths, as the reference does for L > 32."""
+    N = len(strings)
+    if N == 0:
+        return np.zeros(0, np.uint32), 0, 0
+    L = len(strings[0])
+    if L > _lib_max_len():
+        raise ValueError(f"[GPU] This kernel only supports lengths <= {_lib_max_len()}.")
+    if any(len(s) != L for s in strings):
+        raise ValueError("all candidates must have the same length")
+    raw = "".join(strings).encode("latin1")
+    out = np.zeros(N, np.uint32)
+    bad = ctypes.c_int64(-1)
+    st = lib().ig_pack(raw, N, L, L, ptr(out), ctypes.byref(bad))
+    if st != 0:
+        raise ValueError(f"candidate {bad.value} is not a string over '0'..'3'")
+    return out, L, N
+
+
+def _lib_max_len() -> int:
+    return 16
+
+
+def apply_filters(words, L: int, max_run: int, min_gc: float, max_gc: float) -> np.ndarray:
+    w = _words_array(words)
+    keep = np.zeros(len(w), np.uint8)
+    check(lib().ig_filter(ptr(w), len(w), int(L), int(max_run), float(min_gc), float(max_gc), ptr(keep)),
+          "ig_filter")
+    return keep.astype(bool)
+
+
+def solve_edit_distance_cuda(strings, threshold, tile_size=16384, max_gpu_memory_gb=9.0, ctx=None):
+    """Adjacency lists of the ED < threshold graph (list of lists, both
+    directions).  tile_size / max_gpu_memory_gb are accepted for interface
+    parity; the library schedules its own tiles and sizes its workspace."""
+    if len(strings) == 0:
+        return []
+    words, L, _ = pack_sequences(strings)
+    with build_conflict_graph(words, L, int(threshold), ctx) as g:
+        return g.adj_list()
+
+
+def fill_adj_list_gpu(candidates, min_ed: int, ctx=None):
+    """FillAdjListGPU: returns (ConflictGraph, matrixOnesNum)."""
+    words, L, _ = pack_sequences(list(candidates))
+    g = build_conflict_graph(words, max(L, 1), int(min_ed), ctx)
+    return g, g.matrix_ones_num
+
+
+def solve_independent_set(candidates, min_ed: int, thread_num: int = 1, ctx=None):
+    """SolveIndependentSet: the codebook strings in selection order.
+    thread_num selects the neighbour order of the reference's FillAdjList
+    with that many threads (1 = the sorted order of the GPU-path loader)."""
+    cands = list(candidates)
+    if len(cands) == 0:
+        return []
+    if len(cands) == 1:
+        return cands
+    words, L, _ = pack_sequences(cands)
+    order, _ = solve(words, L, min_ed, thread_num, ctx)
+    return [cands[i] for i in order.tolist()]
+
+
+def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
+    """True iff no pair of `vecs` is closer than min_ed."""
+    if len(vecs) < 2:
+        return True
+    words, L, _ = pack_sequences(list(vecs))
+    return count_conflicts(words, L, min_ed, ctx) == 0
+
+
+__all__ = [
+    "Context", "ConflictGraph", "IndexGenError", "build_conflict_graph", "count_conflicts",
+    "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
+    "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context",
+]

@@ -1,0 +1,188 @@
+"""Seeded candidate sets for the conflict-graph workloads.
+
+These produce the INPUT of the accelerated path (2-bit packed words, character
+p at bits 2p..2p+1).  They restate the reference's candidate sources where a
+workload names one:
+
+* ``uniform_words``  -- i.i.d. uniform 4-ary strings (numpy PCG64), the stand-in
+  for the reference's ``Random`` method (src/CandidateGenerator.cpp:410-446),
+  which seeds from std::random_device and so cannot be replayed.
+* ``linear_code_words`` -- all codewords of the shortened GF(4) Hamming code
+  [n, n-3, 3] in the order src/Candidates/LinearCodes.cpp:225-289 emits them:
+  data vectors counted in base 4 with the last digit fastest (src/Utils.cpp:525-542),
+  encoded by the permuted generator matrix, plus the bias (coset) vector.
+* ``vt16_words`` -- seeded uniform draws of the quaternary VT-style code
+  sum(i*x_i) = 0 (mod 17), sum(x_i) = 0 (mod 4) used by the large sparse graph.
+* ``filter_words`` -- MaxRun / GC-content filters with the reference's double
+  comparisons (src/CandidateGenerator.cpp:24-50, src/Utils.cpp:420-462).
+"""
+from __future__ import annotations
+
+import itertools
+
+import numpy as np
+
+# GF(4) = {0, 1, a, a^2} coded 0,1,2,3 with a^2 = a + 1: addition is XOR of the
+# 2-bit codes, multiplication goes through discrete logs.
+_LOG = {1: 0, 2: 1, 3: 2}
+_EXP = [1, 2, 3]
+
+
+def gf4_mul(a: int, b: int) -> int:
+    if a == 0 or b == 0:
+        return 0
+    return _EXP[(_LOG[a] + _LOG[b]) % 3]
+
+
+def hamming_parity_rows() -> list[tuple[int, int, int]]:
+    """Parity rows of the systematic GF(4) Hamming code of length 21.
+
+    One normalised representative (first non-zero coordinate 1) of every point
+    of PG(2,4) that is not a unit vector, in lexicographic order.  Appending
+    them to the identity gives the [21,18,3] generator that
+    src/Candidates/GenMat.cpp:9-33 tabulates.
+    """
+    rows = []
+    for v in itertools.product(range(4), repeat=3):
+        nz = [x for x in v if x]
+        if len(nz) >= 2 and nz[0] == 1:
+            rows.append(v)
+    assert len(rows) == 18
+    return rows
+
+
+def hamming_generator(n: int) -> np.ndarray:
+    """Generator of the [21,18,3] code shortened to length n (4 <= n <= 21).
+
+    Shortening drops the first 21-n data rows and coordinates, as
+    src/Candidates/LinearCodes.cpp:118-136 / :160-166 do.
+    """
+    if not 4 <= n <= 21:
+        raise ValueError("length must be in 4..21")
+    full = np.zeros((18, 21), np.int64)
+    full[:, :18] = np.eye(18, dtype=np.int64)
+    full[:, 18:] = np.array(hamming_parity_rows(), np.int64)
+    d = 21 - n
+    return full[d:, d:]
+
+
+def linear_code_words(n: int, bias, row_perm=None, col_perm=None) -> np.ndarray:
+    """All 4^(n-3) codewords (+ bias) as packed words, in the reference's order."""
+    G = hamming_generator(n)
+    k = G.shape[0]
+    if col_perm is not None:
+        G = G[:, list(col_perm)]
+    if row_perm is not None:
+        G = G[list(row_perm), :]
+    # data vectors in base-4 counting order, last digit fastest
+    idx = np.arange(4 ** k, dtype=np.int64)
+    data = (idx[:, None] >> (2 * np.arange(k - 1, -1, -1, dtype=np.int64))[None, :]) & 3
+    code = np.zeros((len(idx), n), np.int64)
+    mul = np.array([[gf4_mul(a, b) for b in range(4)] for a in range(4)], np.int64)
+    for i in range(k):
+        code ^= mul[data[:, i][:, None], G[i][None, :]]
+    code ^= np.asarray(bias, np.int64)[None, :]
+    return pack_digits(code)
+
+
+def pack_digits(digits) -> np.ndarray:
+    d = np.asarray(digits, dtype=np.uint32)
+    L = d.shape[1]
+    return (d << (2 * np.arange(L, dtype=np.uint32))[None, :]).sum(axis=1, dtype=np.uint64).astype(np.uint32)
+
+
+def unpack_digits(words, L: int) -> np.ndarray:
+    w = np.asarray(words, dtype=np.uint32)
+    return ((w[:, None] >> (2 * np.arange(L, dtype=np.uint32))[None, :]) & 3).astype(np.uint8)
+
+
+def to_strings(words, L: int) -> list[str]:
+    d = unpack_digits(words, L) + ord("0")
+    return [bytes(r).decode("ascii") for r in d]
+
+
+def from_strings(strings) -> np.ndarray:
+    if len(strings) == 0:
+        return np.zeros(0, np.uint32)
+    L = len(strings[0])
+    raw = np.frombuffer("".join(strings).encode("latin1"), np.uint8).reshape(len(strings), L)
+    if np.any((raw < 48) | (raw > 51)):
+        raise ValueError("candidates must be strings over '0'..'3'")
+    return pack_digits(raw - 48)
+
+
+def filter_words(words, L: int, max_run: int = 3, min_gc: float = 0.3, max_gc: float = 0.7) -> np.ndarray:
+    """Boolean keep-mask with the reference filter semantics."""
+    d = unpack_digits(words, L).astype(np.int64)
+    keep = np.ones(len(d), bool)
+    if max_run > 0:
+        run = np.ones(len(d), np.int64)
+        best = np.ones(len(d), np.int64)
+        for p in range(1, L):
+            same = d[:, p] == d[:, p - 1]
+            run = np.where(same, run + 1, 1)
+            best = np.maximum(best, run)
+        keep &= best <= max_run
+    if min_gc > 0 or max_gc > 0:
+        gc = ((d == 1) | (d == 2)).sum(axis=1).astype(np.float64) / float(L)
+        keep &= (gc >= min_gc) & (gc <= max_gc)
+    return keep
+
+
+def uniform_words(count: int, L: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return pack_digits(rng.integers(0, 4, size=(count, L)))
+
+
+def uniform_filtered(count: int, L: int, seed: int, **flt) -> np.ndarray:
+    """`count` uniform draws, then the filters (order preserved)."""
+    w = uniform_words(count, L, seed)
+    return w[filter_words(w, L, **flt)]
+
+
+def uniform_until(target: int, L: int, seed: int, **flt) -> np.ndarray:
+    """Draw uniform strings in seeded batches until `target` survive the filters."""
+    rng = np.random.default_rng(seed)
+    out = []
+    have = 0
+    while have < target:
+        w = pack_digits(rng.integers(0, 4, size=(max(4096, target), L)))
+        w = w[filter_words(w, L, **flt)]
+        out.append(w)
+        have += len(w)
+    return np.concatenate(out)[:target]
+
+
+def vt16_words(target: int, seed: int, max_run: int = 3, min_gc: float = 0.3, max_gc: float = 0.7) -> np.ndarray:
+    """`target` filtered words of sum(i*x_i)=0 mod 17, sum(x_i)=0 mod 4 (n=16)."""
+    L = 16
+    rng = np.random.default_rng(seed)
+    out = []
+    have = 0
+    pos = np.arange(1, L + 1, dtype=np.int64)
+    while have < target:
+        d = rng.integers(0, 4, size=(1 << 22, L))
+        ok = ((d * pos).sum(axis=1) % 17 == 0) & (d.sum(axis=1) % 4 == 0)
+        w = pack_digits(d[ok])
+        w = w[filter_words(w, L, max_run, min_gc, max_gc)]
+        out.append(w)
+        have += len(w)
+    return np.concatenate(out)[:target]
+
+
+# The coset vector the reference's LinearCode generator draws for n=12 with
+# biasMode=random and randomSeed=20251203 (mt19937 + uniform_int_distribution,
+# src/CandidateGenerator.cpp:81-96); pinned by the golden fixture.
+LINEAR12_SEED = 20251203
+LINEAR12_BIAS = (1, 0, 0, 2, 1, 3, 3, 0, 1, 0, 3, 0)
+
+
+def linear12_candidates() -> np.ndarray:
+    """The single-large-job workload: [12,9,3] GF(4) code + seeded coset, filtered."""
+    w = linear_code_words(12, LINEAR12_BIAS)
+    return w[filter_words(w, 12, 3, 0.3, 0.7)]
+
+
+def uniform11_candidates() -> np.ndarray:
+    """The CPU-runnable workload: 20,000 uniform n=11 strings (seed 12345), filtered."""
+    return uniform_filtered(20000, 11, 12345, max_run=3, min_gc=0.3, max_gc=0.7)

@@ -1,0 +1,142 @@
+"""ctypes front end of the CPU oracle (oracle/ig_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+as the checker, and by the ``cpu_baseline`` leg of bench.py.  The product
+package never imports it.
+
+The C library restates the reference path (edge predicate of
+include/EditDistance.hpp:368-372, neighbour order of src/SparseMat.cpp:599-609,
+greedy of src/SparseMat.cpp:81-266/679-731) and is pinned against golden
+vectors produced by the reference's own C++ code (tests/golden/).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libigoracle.so")
+_lib = None
+
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle library with gcc (Makefile beside this file)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(
+            os.path.join(_HERE, "ig_oracle.c")
+        ):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.igo_pack.restype = ctypes.c_int64
+        L.igo_pack.argtypes = [ctypes.c_char_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64, _u32p]
+        L.igo_lev_dp.restype = ctypes.c_int
+        L.igo_lev_dp.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]
+        L.igo_lev_myers.restype = ctypes.c_int
+        L.igo_lev_myers.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int]
+        L.igo_filter.restype = None
+        L.igo_filter.argtypes = [_u32p, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, _u8p]
+        L.igo_conflict_upper.restype = ctypes.c_int
+        L.igo_conflict_upper.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         _i64p, ctypes.c_void_p]
+        L.igo_adjacency.restype = None
+        L.igo_adjacency.argtypes = [_i64p, _i32p, ctypes.c_int32, ctypes.c_int, _i64p, _i32p]
+        L.igo_greedy.restype = ctypes.c_int32
+        L.igo_greedy.argtypes = [_i64p, _i32p, ctypes.c_int32, _i32p]
+        _lib = L
+    return _lib
+
+
+def pack(strings) -> np.ndarray:
+    """'0'..'3' strings of one length -> uint32 words (char p at bits 2p..2p+1)."""
+    n = len(strings)
+    if n == 0:
+        return np.zeros(0, np.uint32)
+    L = len(strings[0])
+    raw = "".join(strings).encode("latin1")
+    out = np.zeros(n, np.uint32)
+    bad = lib().igo_pack(raw, n, L, L, out)
+    if bad >= 0:
+        raise ValueError(f"row {bad} is not a '0'..'3' string of length {L}")
+    return out
+
+
+def unpack(words, L: int):
+    w = np.asarray(words, dtype=np.uint32)
+    digits = (w[:, None] >> (2 * np.arange(L, dtype=np.uint32))[None, :]) & 3
+    return ["".join(map(str, row)) for row in digits.tolist()]
+
+
+def lev(a: int, b: int, L: int, method: str = "myers") -> int:
+    f = lib().igo_lev_myers if method == "myers" else lib().igo_lev_dp
+    return int(f(int(a), int(b), L))
+
+
+def filter_mask(words, L: int, max_run: int, min_gc: float, max_gc: float) -> np.ndarray:
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    keep = np.zeros(len(w), np.uint8)
+    lib().igo_filter(w, len(w), L, max_run, min_gc, max_gc, keep)
+    return keep.astype(bool)
+
+
+def conflict_upper(words, L: int, min_ed: int, threads: int | None = None):
+    """Upper CSR (row_ptr int64[n+1], cols int32[nnz]) of pairs i<j with ED < min_ed."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    n = len(w)
+    threads = threads or max(1, len(os.sched_getaffinity(0)))
+    row_ptr = np.zeros(n + 1, np.int64)
+    # one pass collects the columns per thread and assembles them in place
+    cols_holder = np.zeros(0, np.int32)
+    rc = lib().igo_conflict_upper(w, n, L, min_ed, threads, row_ptr, None)
+    if rc != 0:
+        raise MemoryError("oracle conflict_upper failed")
+    nnz = int(row_ptr[-1])
+    cols_holder = np.zeros(max(nnz, 1), np.int32)
+    rc = lib().igo_conflict_upper(w, n, L, min_ed, threads, row_ptr, cols_holder.ctypes.data)
+    if rc != 0:
+        raise MemoryError("oracle conflict_upper failed")
+    return row_ptr, cols_holder[:nnz]
+
+
+def adjacency(row_ptr, cols, n: int, order_threads: int = 1):
+    row_ptr = np.ascontiguousarray(row_ptr, dtype=np.int64)
+    cols = np.ascontiguousarray(cols, dtype=np.int32)
+    nnz = int(row_ptr[-1])
+    adj_ptr = np.zeros(n + 1, np.int64)
+    adj = np.zeros(max(2 * nnz, 1), np.int32)
+    lib().igo_adjacency(row_ptr, cols if len(cols) else np.zeros(1, np.int32), n, order_threads, adj_ptr, adj)
+    return adj_ptr, adj[: 2 * nnz]
+
+
+def greedy(adj_ptr, adj, n: int) -> np.ndarray:
+    adj_ptr = np.ascontiguousarray(adj_ptr, dtype=np.int64)
+    adj = np.ascontiguousarray(adj, dtype=np.int32)
+    order = np.zeros(max(n, 1), np.int32)
+    cnt = lib().igo_greedy(adj_ptr, adj if len(adj) else np.zeros(1, np.int32), n, order)
+    return order[:cnt]
+
+
+def codebook(row_ptr, cols, n: int, order_threads: int = 1) -> np.ndarray:
+    ap, a = adjacency(row_ptr, cols, n, order_threads)
+    return greedy(ap, a, n)
+
+
+def pairs_from_csr(row_ptr, cols) -> np.ndarray:
+    """(u, v) int32 pairs, u < v, rows ascending: the reference's binary edge-file layout."""
+    row_ptr = np.asarray(row_ptr, dtype=np.int64)
+    rows = np.repeat(np.arange(len(row_ptr) - 1, dtype=np.int32), np.diff(row_ptr))
+    return np.stack([rows, np.asarray(cols, dtype=np.int32)], axis=1)
