@@ -365,12 +365,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subset", type=int, default=0,
+                    help="use a seeded random subset of this many words (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     wl = workload(args.workload)
+    if args.subset and args.subset < len(wl["words"]):
+        rng = np.random.default_rng(4321)
+        wl["words"] = wl["words"][np.sort(rng.choice(len(wl["words"]), args.subset, replace=False))]
+        wl["name"] += f"_subset{args.subset}"
     if args.impl == "reference":
         run_reference(args, wl, rank)
         return

@@ -4,13 +4,14 @@
 // (:20-226, :278-446) and the Python edge writer (src/gpu_graph_generator.py:49-77).
 //
 // Pipeline for one job of n words of length L and threshold d (edge iff ED < d):
-//   prep_selectors  word -> 16-byte PRMT selector stream (one byte per character)
+//   prep_units      words -> PRMT selector streams, two columns per unit for L <= 15
 //   pair_kernel<L>  persistent CTAs take (row band, column segment) items from an
 //                   atomic queue; 256 rows per band live in registers as two PRMT
 //                   pools of Myers Peq masks; column tiles of the segment are
 //                   staged into shared memory by cp.async.bulk (TMA bulk copy, no
 //                   multicast) with a two-slot mbarrier pipeline; each thread runs
-//                   the 32-bit Myers recurrence per (row, column) and emits hits
+//                   the 32-bit Myers recurrence on two columns at once (two
+//                   16-bit lanes, L <= 15) or one (L = 16) and emits hits
 //                   through warp ballot + one atomic per warp as
 //                   (row, col, rank-in-(row,segment), segment) records, plus a
 //                   per-(row, segment) count.
@@ -81,31 +82,79 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 // ---------------------------------------------------------------------------
-// Selector stream: byte k = (2c) | (2c+1) << 4 for character c at position k.
-// __byte_perm(P01, P23, sel >> 8k) then returns Peq[c] in its low 16 bits,
-// where P01 = Peq0 | Peq1 << 16 and P23 = Peq2 | Peq3 << 16.
+// Column streams.  A column "unit" is what a thread tests against its row in
+// one inner step:
+//  * L <= 15: two columns, one per 16-bit lane of a 32-bit word.  Stored as 16
+//    32-bit selector words, one per character position; bits 0..15 hold the
+//    PRMT nibbles (2a, 2a+1, 2b, 2b+1) of the two columns' characters a, b.
+//  * L = 16: one column.  Stored as 16-bit selectors (2c, 2c+1, -, -), two
+//    character positions per 32-bit word.
+// With P01 = Peq0 | Peq1 << 16 and P23 = Peq2 | Peq3 << 16 (the row's Myers
+// match masks), __byte_perm(P01, P23, sel) returns Peq[a] | Peq[b] << 16
+// (resp. Peq[c] in the low half).
 // ---------------------------------------------------------------------------
-__global__ void prep_selectors(const uint32_t *__restrict__ words, int32_t n, int len, uint4 *__restrict__ sel)
+template <int L>
+struct Unit {
+    static constexpr bool kTwo = L <= 15;
+    static constexpr int kCols = kTwo ? 2 : 1;      // columns per unit
+    static constexpr int kVec = kTwo ? 4 : 2;       // uint4 per unit in the stream
+    static constexpr int kUsed = (L + 3) / 4;       // uint4 read per two-lane unit
+    static constexpr int kBytes = kVec * 16;
+    static constexpr int kTileUnits = kTileCols / kCols;
+};
+
+
+__device__ __forceinline__ uint32_t nib(uint32_t c) { return (2u * c) | ((2u * c + 1u) << 4); }
+
+// units of two columns (L <= 15): out[4*p .. 4*p+3] for columns 2p, 2p+1
+__global__ void prep_units2(const uint32_t *__restrict__ words, int32_t n, int len, uint4 *__restrict__ out)
+{
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= ((int64_t)n + 1) / 2)
+        return;
+    const uint32_t wa = words[2 * p];
+    const uint32_t wb = (2 * p + 1 < n) ? words[2 * p + 1] : wa;
+    uint32_t o[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        o[k] = 0u;
+        if (k < len)
+            o[k] = nib((wa >> (2 * k)) & 3u) | (nib((wb >> (2 * k)) & 3u) << 8);
+    }
+    uint4 *dst = out + 4 * p;
+    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    dst[2] = make_uint4(o[8], o[9], o[10], o[11]);
+    dst[3] = make_uint4(o[12], o[13], o[14], o[15]);
+}
+
+// units of one column (L = 16): out[2*i .. 2*i+1], two positions per word
+__global__ void prep_units1(const uint32_t *__restrict__ words, int32_t n, int len, uint4 *__restrict__ out)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n)
         return;
     const uint32_t w = words[i];
-    uint32_t o[4] = {0u, 0u, 0u, 0u};
+    uint32_t o[8];
 #pragma unroll
-    for (int k = 0; k < IG_MAX_LEN; ++k) {
-        if (k < len) {
-            const uint32_t c = (w >> (2 * k)) & 3u;
-            o[k >> 2] |= ((2u * c) | ((2u * c + 1u) << 4)) << (8 * (k & 3));
-        }
+    for (int j = 0; j < 8; ++j) {
+        o[j] = 0u;
+        if (2 * j < len)
+            o[j] |= nib((w >> (4 * j)) & 3u);
+        if (2 * j + 1 < len)
+            o[j] |= nib((w >> (4 * j + 2)) & 3u) << 16;
     }
-    sel[i] = make_uint4(o[0], o[1], o[2], o[3]);
+    uint4 *dst = out + 2 * i;
+    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
 }
 
 template <int L>
 __device__ __forceinline__ void row_pools(uint32_t w, uint32_t &p01, uint32_t &p23)
 {
-    uint32_t m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+    // In the two-lane layout every mask carries bit 15, the lane separator.
+    constexpr uint32_t sep = Unit<L>::kTwo ? 0x8000u : 0u;
+    uint32_t m0 = sep, m1 = sep, m2 = sep, m3 = sep;
 #pragma unroll
     for (int k = 0; k < L; ++k) {
         const uint32_t c = (w >> (2 * k)) & 3u;
@@ -119,38 +168,91 @@ __device__ __forceinline__ void row_pools(uint32_t w, uint32_t &p01, uint32_t &p
     p23 = m2 | (m3 << 16);
 }
 
-// Levenshtein distance of the row pattern (pools p01/p23) and one column text
-// (selector stream s): Myers' bit-vector recurrence (global alignment: the
-// horizontal delta entering row 0 is +1), distance read at the end of the text
-// as L + popc(PV) - popc(MV) over the L pattern bits.  Bits >= L of Eq carry
-// other characters' masks; they never reach bits < L (carries and shifts only
-// move upwards), so no masking is needed inside the loop.
-template <int L>
-__device__ __forceinline__ int myers_distance(uint32_t p01, uint32_t p23, const uint4 s)
+// Integer multiply-add with an operand the compiler cannot see as a constant,
+// so it stays an IMAD on the FMA pipe instead of a shift/add on the ALU pipe
+// (the ALU pipe is the one the logic operations saturate).
+__device__ __forceinline__ uint32_t imad(uint32_t a, uint32_t b, uint32_t c)
 {
-    const uint32_t sw[4] = {s.x, s.y, s.z, s.w};
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+// Myers' bit-vector recurrence in Hyyro's formulation (global alignment: the
+// horizontal delta entering row 0 is +1):
+//   Xv = Eq | Mv;  Xh = (((Eq & Pv) + Pv) ^ Pv) | Eq
+//   Ph = Mv | ~(Xh | Pv);  Mh = Pv & Xh;  Ph <<= 1 (+1);  Mh <<= 1
+//   Pv = Mh | ~(Xv | Ph);  Mv = Ph & Xv
+// and the distance read at the end of the text as L + popc(Pv) - popc(Mv) over
+// the pattern rows.  The add and both shifts run as IMADs.
+//
+// Two-lane form (L <= 15): lane 0 = bits 0..14, lane 1 = bits 16..30, 15
+// pattern rows each (rows >= L never match); bits 15 and 31 separate them.
+// Invariants that keep the lanes independent:
+//   Eq has both separator bits set (every Peq mask carries bit 15),
+//   Pv and Mv have both separator bits clear,
+//   Mh has the top row (bits 14, 30) clear -- it could only shift into a separator.
+// Then the carry of (Eq&Pv)+Pv stops at bit 15 (both addends are 0 there),
+// Ph has bit 15 clear (Xh has it set, Mv not), so Ph*2 + 0x00010001 injects the
+// +1 boundary into row 0 of both lanes without a carry, Mh*2 brings 0 into row 0
+// of lane 1, and the new Pv has bit 15 clear because Xv has it set.
+template <int L>
+__device__ __forceinline__ void myers_two(uint32_t p01, uint32_t p23, const uint32_t (&sel)[16], uint32_t one,
+                                          uint32_t two, int lim, bool &h0, bool &h1)
+{
+    uint32_t pv = 0x7fff7fffu, mv = 0u;
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+        const uint32_t eq = __byte_perm(p01, p23, sel[k]);
+        const uint32_t xv = eq | mv;
+        const uint32_t s = imad(eq & pv, one, pv);
+        const uint32_t xh = (s ^ pv) | eq;
+        const uint32_t ph = mv | ~(xh | pv);
+        const uint32_t mh = pv & xh & 0xbfffbfffu;
+        const uint32_t ph2 = imad(ph, two, 0x00010001u);
+        const uint32_t mh2 = imad(mh, two, 0u);
+        pv = mh2 | ~(xv | ph2);
+        mv = ph2 & xv & 0x7fff7fffu;
+    }
+    constexpr uint32_t M0 = (1u << L) - 1u;
+    constexpr uint32_t M1 = M0 << 16;
+    h0 = (__popc(pv & M0) - __popc(mv & M0)) < lim;
+    h1 = (__popc(pv & M1) - __popc(mv & M1)) < lim;
+}
+
+// One-lane form (L = 16): bits >= 16 of Eq hold other masks' bytes; carries
+// and shifts only move upwards, so they never reach the pattern rows.
+template <int L>
+__device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint32_t (&sel)[8], uint32_t one,
+                                          uint32_t two, uint32_t hi, int lim)
+{
     uint32_t pv = 0xffffffffu, mv = 0u;
 #pragma unroll
     for (int k = 0; k < L; ++k) {
-        const uint32_t sel = sw[k >> 2] >> (8 * (k & 3));
-        const uint32_t eq = __byte_perm(p01, p23, sel);
-        const uint32_t x = eq | mv;
-        const uint32_t d0 = (((x & pv) + pv) ^ pv) | x;
-        const uint32_t hn = pv & d0;
-        const uint32_t hp = mv | ~(pv | d0);
-        const uint32_t x2 = (hp << 1) | 1u;
-        mv = x2 & d0;
-        pv = (hn << 1) | ~(x2 | d0);
+        const uint32_t sw = (k & 1) ? __umulhi(sel[k >> 1], hi) : sel[k >> 1];
+        const uint32_t eq = __byte_perm(p01, p23, sw);
+        const uint32_t xv = eq | mv;
+        const uint32_t s = imad(eq & pv, one, pv);
+        const uint32_t xh = (s ^ pv) | eq;
+        const uint32_t ph = mv | ~(xh | pv);
+        const uint32_t mh = pv & xh;
+        const uint32_t ph2 = imad(ph, two, 1u);
+        const uint32_t mh2 = imad(mh, two, 0u);
+        pv = mh2 | ~(xv | ph2);
+        mv = ph2 & xv;
     }
     constexpr uint32_t M = (L >= 32) ? 0xffffffffu : ((1u << L) - 1u);
-    return L + __popc(pv & M) - __popc(mv & M);
+    return (__popc(pv & M) - __popc(mv & M)) < lim;
 }
 
 struct PairArgs {
-    const uint4 *sel;
+    const uint4 *units;
     const uint32_t *words;
     int32_t n;
-    int min_ed;
+    int lim;          // min_ed - L: a pair is an edge iff popc(Pv) - popc(Mv) < lim
+    uint32_t one;     // 1 and 2 (and 1 << 16) as opaque operands for imad / umulhi
+    uint32_t two;
+    uint32_t hi;
     int seg_shift;
     int nseg;
     int bands_per_seg;
@@ -190,48 +292,65 @@ __device__ __forceinline__ void emit_hit(const PairArgs &a, bool hit, uint32_t r
     }
 }
 
-// One staged tile of nc columns starting at column c0.  CHECK adds the
-// strict-upper-triangle test (col > row) and the row < n test; it is only
-// needed on the diagonal items and on the last (partial) band.
+// One staged tile of nu units whose first column is c0.  CHECK adds the
+// strict-upper-triangle test (col > row), row < n and col < n; it is only
+// needed on diagonal items, the last (partial) band and an odd last column.
 template <int L, bool CHECK>
-__device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, int nc, int32_t c0, int32_t row,
+__device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, int nu, int32_t c0, int32_t row,
                                           bool row_ok, uint32_t p01, uint32_t p23, uint32_t seg, uint32_t &rank,
                                           int lane)
 {
-    int j = 0;
-    for (; j + 1 < nc; j += 2) {
-        const uint4 s0 = tile[j];
-        const uint4 s1 = tile[j + 1];
-        const int e0 = myers_distance<L>(p01, p23, s0);
-        const int e1 = myers_distance<L>(p01, p23, s1);
-        bool h0 = e0 < a.min_ed;
-        bool h1 = e1 < a.min_ed;
-        if (CHECK) {
-            h0 = h0 && row_ok && (c0 + j > row);
-            h1 = h1 && row_ok && (c0 + j + 1 > row);
+    using U = Unit<L>;
+    for (int u = 0; u < nu; ++u) {
+        const uint4 *src = tile + u * U::kVec;
+        if constexpr (U::kTwo) {
+            uint32_t sel[16];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                if (v < U::kUsed) {
+                    const uint4 q = src[v];
+                    sel[4 * v] = q.x;
+                    sel[4 * v + 1] = q.y;
+                    sel[4 * v + 2] = q.z;
+                    sel[4 * v + 3] = q.w;
+                } else {
+                    sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
+                }
+            }
+            bool h0, h1;
+            myers_two<L>(p01, p23, sel, a.one, a.two, a.lim, h0, h1);
+            const int32_t col = c0 + 2 * u;
+            if (CHECK) {
+                h0 = h0 && row_ok && (col > row) && (col < a.n);
+                h1 = h1 && row_ok && (col + 1 > row) && (col + 1 < a.n);
+            }
+            if (__any_sync(kFull, h0 || h1)) {
+                emit_hit(a, h0, (uint32_t)row, (uint32_t)col, seg, rank, lane);
+                emit_hit(a, h1, (uint32_t)row, (uint32_t)(col + 1), seg, rank, lane);
+            }
+        } else {
+            uint32_t sel[8];
+            const uint4 q0 = src[0];
+            const uint4 q1 = src[1];
+            sel[0] = q0.x; sel[1] = q0.y; sel[2] = q0.z; sel[3] = q0.w;
+            sel[4] = q1.x; sel[5] = q1.y; sel[6] = q1.z; sel[7] = q1.w;
+            bool h0 = myers_one<L>(p01, p23, sel, a.one, a.two, a.hi, a.lim);
+            const int32_t col = c0 + u;
+            if (CHECK)
+                h0 = h0 && row_ok && (col > row);
+            if (__any_sync(kFull, h0))
+                emit_hit(a, h0, (uint32_t)row, (uint32_t)col, seg, rank, lane);
         }
-        if (__any_sync(kFull, h0 || h1)) {
-            emit_hit(a, h0, (uint32_t)row, (uint32_t)(c0 + j), seg, rank, lane);
-            emit_hit(a, h1, (uint32_t)row, (uint32_t)(c0 + j + 1), seg, rank, lane);
-        }
-    }
-    if (j < nc) {
-        const int e0 = myers_distance<L>(p01, p23, tile[j]);
-        bool h0 = e0 < a.min_ed;
-        if (CHECK)
-            h0 = h0 && row_ok && (c0 + j > row);
-        if (__any_sync(kFull, h0))
-            emit_hit(a, h0, (uint32_t)row, (uint32_t)(c0 + j), seg, rank, lane);
     }
 }
 
 template <int L>
 __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
 {
-    __shared__ __align__(128) uint4 tile[2][kTileCols];
+    using U = Unit<L>;
+    __shared__ __align__(128) uint4 tile[2][U::kTileUnits * U::kVec];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ long long item_sh;
-    __shared__ int abort_sh;  // set when a wait gave up; read by the host via status
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -239,7 +358,6 @@ __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_fence_init();
-        abort_sh = 0;
     }
     __syncthreads();
     uint32_t parity = 0u;  // bit b: phase parity of slot b
@@ -277,19 +395,23 @@ __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
         const bool row_ok = row < a.n;
         uint32_t p01, p23;
         row_pools<L>(a.words[row_ok ? row : 0], p01, p23);
+        // c_lo is a multiple of 256 (segments and bands are), so units never
+        // straddle a segment
         const int32_t c_lo = (int32_t)max((long long)seg << a.seg_shift, (long long)row0);
         const int32_t c_hi = (int32_t)min((long long)(seg + 1) << a.seg_shift, (long long)a.n);
         const long long row_end = (long long)row0 + kBandRows;
-        const bool check = ((long long)c_lo < row_end) || (row_end > (long long)a.n);
+        const bool check = ((long long)c_lo < row_end) || (row_end > (long long)a.n) ||
+                           (U::kCols == 2 && (c_hi & 1));
         const int ntiles = (c_hi - c_lo + kTileCols - 1) / kTileCols;
         uint32_t rank = 0;
 
         if (tid == 0) {
             for (int t = 0; t < 2 && t < ntiles; ++t) {
                 const int32_t c0 = c_lo + t * kTileCols;
-                const uint32_t bytes = (uint32_t)min(kTileCols, c_hi - c0) * 16u;
+                const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
+                const uint32_t bytes = (uint32_t)nu * U::kBytes;
                 mbar_arrive_expect_tx(&bar[t], bytes);
-                bulk_g2s(&tile[t][0], a.sel + c0, bytes, &bar[t]);
+                bulk_g2s(&tile[t][0], a.units + (size_t)(c0 / U::kCols) * U::kVec, bytes, &bar[t]);
             }
         }
         for (int t = 0; t < ntiles; ++t) {
@@ -305,25 +427,24 @@ __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
             parity ^= 1u << b;
             // uniform decision: every thread leaves together if any gave up
             if (__syncthreads_or(timed_out)) {
-                if (tid == 0) {
+                if (tid == 0)
                     atomicExch(a.status, kStatusTimeout);
-                    abort_sh = 1;
-                }
                 aborted = true;
                 break;
             }
             const int32_t c0 = c_lo + t * kTileCols;
-            const int nc = min(kTileCols, c_hi - c0);
+            const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
             if (check)
-                tile_pass<L, true>(a, tile[b], nc, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
+                tile_pass<L, true>(a, tile[b], nu, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
             else
-                tile_pass<L, false>(a, tile[b], nc, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
+                tile_pass<L, false>(a, tile[b], nu, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
             __syncthreads();
             if (tid == 0 && t + 2 < ntiles) {
                 const int32_t cn = c_lo + (t + 2) * kTileCols;
-                const uint32_t bytes = (uint32_t)min(kTileCols, c_hi - cn) * 16u;
+                const int nun = (min(kTileCols, c_hi - cn) + U::kCols - 1) / U::kCols;
+                const uint32_t bytes = (uint32_t)nun * U::kBytes;
                 mbar_arrive_expect_tx(&bar[b], bytes);
-                bulk_g2s(&tile[b][0], a.sel + cn, bytes, &bar[b]);
+                bulk_g2s(&tile[b][0], a.units + (size_t)(cn / U::kCols) * U::kVec, bytes, &bar[b]);
             }
         }
         if (aborted)
@@ -529,7 +650,10 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
 {
     cudaStream_t st = ctx->stream;
     ig_status s;
-    if ((s = ensure(ctx, ctx->sel, (size_t)n * sizeof(uint4), "selector streams")) != IG_OK)
+    const bool two = len <= 15;
+    const size_t unit_bytes = two ? 64 : 32;
+    const size_t units = two ? ((size_t)n + 1) / 2 : (size_t)n;
+    if ((s = ensure(ctx, ctx->sel, units * unit_bytes, "column streams")) != IG_OK)
         return s;
     if ((s = ensure(ctx, ctx->counts, (size_t)plan.nseg * (size_t)n * sizeof(uint32_t), "segment counts")) !=
         IG_OK)
@@ -537,17 +661,26 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
     if ((s = ensure(ctx, ctx->flags, 4 * sizeof(unsigned long long), "flags")) != IG_OK)
         return s;
     phase_begin(ctx, IG_PHASE_PREP);
-    prep_selectors<<<(n + 255) / 256, 256, 0, st>>>(d_words, n, len, static_cast<uint4 *>(ctx->sel.ptr));
+    if (two)
+        prep_units2<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(d_words, n, len,
+                                                                     static_cast<uint4 *>(ctx->sel.ptr));
+    else
+        prep_units1<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(d_words, n, len,
+                                                                     static_cast<uint4 *>(ctx->sel.ptr));
     phase_end(ctx, IG_PHASE_PREP);
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
     unsigned long long *flags = static_cast<unsigned long long *>(ctx->flags.ptr);
     IG_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned long long), st));
     PairArgs a;
-    a.sel = static_cast<const uint4 *>(ctx->sel.ptr);
+    a.units = static_cast<const uint4 *>(ctx->sel.ptr);
     a.words = d_words;
     a.n = n;
-    a.min_ed = min_ed;
+    // min_ed <= 0: no pair can be an edge; min_ed > L: every pair is one
+    a.lim = (int)std::max(-64, std::min(64, min_ed - len));
+    a.one = 1u;
+    a.two = 2u;
+    a.hi = 1u << 16;
     a.seg_shift = plan.seg_shift;
     a.nseg = plan.nseg;
     a.bands_per_seg = plan.bands_per_seg;
