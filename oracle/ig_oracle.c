@@ -153,8 +153,26 @@ static void *upper_worker(void *arg)
     return NULL;
 }
 
+static int conflict_upper_impl(const uint32_t *words, int32_t n, int len, int min_ed, int threads,
+                               int64_t *row_ptr, int32_t *cols, int32_t **cols_alloc);
+
 int igo_conflict_upper(const uint32_t *words, int32_t n, int len, int min_ed, int threads, int64_t *row_ptr,
                        int32_t *cols)
+{
+    return conflict_upper_impl(words, n, len, min_ed, threads, row_ptr, cols, NULL);
+}
+
+int igo_conflict_upper_alloc(const uint32_t *words, int32_t n, int len, int min_ed, int threads, int64_t *row_ptr,
+                             int32_t **cols)
+{
+    *cols = NULL;
+    return conflict_upper_impl(words, n, len, min_ed, threads, row_ptr, NULL, cols);
+}
+
+void igo_free(void *p) { free(p); }
+
+static int conflict_upper_impl(const uint32_t *words, int32_t n, int len, int min_ed, int threads,
+                               int64_t *row_ptr, int32_t *cols, int32_t **cols_alloc)
 {
     if (threads < 1)
         threads = 1;
@@ -175,6 +193,11 @@ int igo_conflict_upper(const uint32_t *words, int32_t n, int len, int min_ed, in
     row_ptr[0] = 0;
     for (int32_t i = 0; i < n; i++)
         row_ptr[i + 1] = row_ptr[i] + cnt[i];
+    if (cols_alloc && !fail) {
+        cols = (int32_t *)malloc((size_t)(row_ptr[n] ? row_ptr[n] : 1) * sizeof(int32_t));
+        *cols_alloc = cols;
+        fail = cols == NULL;
+    }
     if (cols && !fail) {
         int64_t *off = (int64_t *)calloc((size_t)threads, sizeof(int64_t));
         for (int32_t i = 0; i < n; i++) {

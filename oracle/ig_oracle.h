@@ -37,6 +37,12 @@ void igo_filter(const uint32_t *words, int64_t n, int len, int max_run, double m
 int igo_conflict_upper(const uint32_t *words, int32_t n, int len, int min_ed, int threads, int64_t *row_ptr,
                        int32_t *cols);
 
+/* Same, in one pass: *cols receives a malloc'ed array of row_ptr[n] entries
+ * (release with igo_free). */
+int igo_conflict_upper_alloc(const uint32_t *words, int32_t n, int len, int min_ed, int threads, int64_t *row_ptr,
+                             int32_t **cols);
+void igo_free(void *p);
+
 /* Neighbour lists in the order src/SparseMat.cpp:599-609 builds them for a
  * FillAdjList run with `order_threads` threads (1 = fully sorted, which is also
  * the order AdjList::FromBinaryFile builds from a row-sorted edge file).

@@ -53,6 +53,11 @@ def lib():
         L.igo_conflict_upper.restype = ctypes.c_int
         L.igo_conflict_upper.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          _i64p, ctypes.c_void_p]
+        L.igo_conflict_upper_alloc.restype = ctypes.c_int
+        L.igo_conflict_upper_alloc.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               _i64p, ctypes.POINTER(ctypes.c_void_p)]
+        L.igo_free.restype = None
+        L.igo_free.argtypes = [ctypes.c_void_p]
         L.igo_adjacency.restype = None
         L.igo_adjacency.argtypes = [_i64p, _i32p, ctypes.c_int32, ctypes.c_int, _i64p, _i32p]
         L.igo_greedy.restype = ctypes.c_int32
@@ -99,17 +104,17 @@ def conflict_upper(words, L: int, min_ed: int, threads: int | None = None):
     n = len(w)
     threads = threads or max(1, len(os.sched_getaffinity(0)))
     row_ptr = np.zeros(n + 1, np.int64)
-    # one pass collects the columns per thread and assembles them in place
-    cols_holder = np.zeros(0, np.int32)
-    rc = lib().igo_conflict_upper(w, n, L, min_ed, threads, row_ptr, None)
+    buf = ctypes.c_void_p()
+    rc = lib().igo_conflict_upper_alloc(w, n, L, min_ed, threads, row_ptr, ctypes.byref(buf))
     if rc != 0:
         raise MemoryError("oracle conflict_upper failed")
     nnz = int(row_ptr[-1])
-    cols_holder = np.zeros(max(nnz, 1), np.int32)
-    rc = lib().igo_conflict_upper(w, n, L, min_ed, threads, row_ptr, cols_holder.ctypes.data)
-    if rc != 0:
-        raise MemoryError("oracle conflict_upper failed")
-    return row_ptr, cols_holder[:nnz]
+    try:
+        cols = np.ctypeslib.as_array(ctypes.cast(buf, ctypes.POINTER(ctypes.c_int32)), shape=(max(nnz, 1),))
+        cols = cols[:nnz].copy()
+    finally:
+        lib().igo_free(buf)
+    return row_ptr, cols
 
 
 def adjacency(row_ptr, cols, n: int, order_threads: int = 1):
