@@ -104,6 +104,14 @@ ig_status ig_graph_upper_csr(const ig_graph *g, int64_t *row_ptr, int32_t *cols)
 ig_status ig_graph_pairs(const ig_graph *g, int32_t *pairs);
 /* Device pointers of the resident upper CSR (valid until ig_graph_free). */
 ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const int32_t **cols);
+/* Symmetric adjacency in the canonical neighbour order m[x] = lower neighbours
+ * ascending, then upper neighbours ascending -- the lists AdjList holds after
+ * FromBinaryFile on the pair file (src/SparseMat.cpp:338-390) or after
+ * FillAdjList with one thread (src/SparseMat.cpp:599-609).  Built on the device
+ * on first request.  adj_ptr[n+1], adj[2*edges] host buffers. */
+ig_status ig_graph_adjacency(ig_graph *g, int64_t *adj_ptr, int32_t *adj);
+/* Device pointers of that adjacency (built on first request). */
+ig_status ig_graph_device_adjacency(ig_graph *g, const int64_t **adj_ptr, const int32_t **adj);
 /* Greedy minimum-degree independent set over the graph, reproducing AdjList's
  * selection order (src/SparseMat.cpp:81-266, :679-731) for neighbour lists
  * assembled as FillAdjList(order_threads) does (src/SparseMat.cpp:599-609);

@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libindexgen_cuda.so")
 EXPORTS = (
     "ig_version", "ig_status_string", "ig_ctx_create", "ig_ctx_destroy", "ig_last_error", "ig_ctx_stream",
     "ig_ctx_reserve", "ig_ctx_launches", "ig_ctx_set_profiling", "ig_ctx_phase_time", "ig_pack", "ig_filter", "ig_graph_build", "ig_graph_free",
-    "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_codebook",
+    "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_adjacency",
+    "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr",
 )
 
@@ -60,6 +61,8 @@ def _declare(L):
         "ig_graph_upper_csr": (_int, [_vp, _vp, _vp]),
         "ig_graph_pairs": (_int, [_vp, _vp]),
         "ig_graph_device_csr": (_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
+        "ig_graph_adjacency": (_int, [_vp, _vp, _vp]),
+        "ig_graph_device_adjacency": (_int, [_vp, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
         "ig_graph_codebook": (_int, [_vp, _int, _vp, ctypes.POINTER(_i32)]),
         "ig_solve": (_int, [_vp, _vp, _i32, _int, _int, _int, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
         "ig_count_conflicts": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),

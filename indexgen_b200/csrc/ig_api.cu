@@ -90,6 +90,10 @@ void release_graph(ig_graph *g)
             cudaFreeAsync(g->d_row_ptr, g->ctx->stream);
         if (g->d_cols)
             cudaFreeAsync(g->d_cols, g->ctx->stream);
+        if (g->d_adj_ptr)
+            cudaFreeAsync(g->d_adj_ptr, g->ctx->stream);
+        if (g->d_adj)
+            cudaFreeAsync(g->d_adj, g->ctx->stream);
         cudaStreamSynchronize(g->ctx->stream);
     }
     delete g;
@@ -99,7 +103,7 @@ ig_status fetch_host(ig_graph *g)
 {
     if (g->host_valid)
         return IG_OK;
-    Ctx *ctx = g->ctx;
+    ig::Ctx *ctx = g->ctx;
     DeviceGuard dg(ctx->device);
     try {
         g->h_row_ptr.resize((size_t)g->n + 1);
@@ -117,6 +121,33 @@ ig_status fetch_host(ig_graph *g)
     if (e != cudaSuccess)
         return cuda_error(ctx, e, "CSR download");
     g->host_valid = true;
+    return IG_OK;
+}
+
+// Canonical symmetric adjacency on the device (built once), then on the host.
+ig_status fetch_adjacency(ig_graph *g, std::vector<int64_t> &ap, std::vector<int32_t> &adj)
+{
+    ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    ig_status s = build_adjacency(ctx, g);
+    if (s != IG_OK)
+        return s;
+    try {
+        ap.resize((size_t)g->n + 1);
+        adj.resize((size_t)std::max<int64_t>(2 * g->edges, 1));
+    } catch (...) {
+        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
+    }
+    cudaError_t e = cudaMemcpyAsync(ap.data(), g->d_adj_ptr, ((size_t)g->n + 1) * sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && g->edges > 0)
+        e = cudaMemcpyAsync(adj.data(), g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, "adjacency download");
     return IG_OK;
 }
 
@@ -183,7 +214,8 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
         return IG_ERR_INPUT;
     {
         ig::DeviceGuard dg(ctx->device);
-        for (ig::DevBuf *b : {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags})
+        for (ig::DevBuf *b :
+             {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags, &ctx->adj_tmp})
             if (b->ptr)
                 cudaFreeAsync(b->ptr, ctx->stream);
         cudaStreamSynchronize(ctx->stream);
@@ -361,15 +393,62 @@ ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const 
     return IG_OK;
 }
 
+ig_status ig_graph_adjacency(ig_graph *g, int64_t *adj_ptr, int32_t *adj)
+{
+    if (!g || !adj_ptr || (g->edges > 0 && !adj))
+        return IG_ERR_INPUT;
+    ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    ig_status s = ig::build_adjacency(ctx, g);
+    if (s != IG_OK)
+        return s;
+    cudaError_t e = cudaMemcpyAsync(adj_ptr, g->d_adj_ptr, ((size_t)g->n + 1) * sizeof(int64_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess && g->edges > 0)
+        e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess)
+        return ig::cuda_error(ctx, e, "adjacency download");
+    return IG_OK;
+}
+
+ig_status ig_graph_device_adjacency(ig_graph *g, const int64_t **adj_ptr, const int32_t **adj)
+{
+    if (!g || !adj_ptr || !adj)
+        return IG_ERR_INPUT;
+    ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    ig_status s = ig::build_adjacency(ctx, g);
+    if (s != IG_OK)
+        return s;
+    *adj_ptr = g->d_adj_ptr;
+    *adj = g->d_adj;
+    return IG_OK;
+}
+
 ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int32_t *count)
 {
     if (!g || !count || order_threads < 1 || (g->n > 0 && !order))
         return IG_ERR_INPUT;
-    ig_status s = ig::fetch_host(g);
-    if (s != IG_OK)
-        return s;
     try {
-        *count = ig::greedy_from_upper(g->h_row_ptr.data(), g->h_cols.data(), g->n, order_threads, order);
+        if (order_threads == 1) {
+            // canonical order: lists come ready from the device
+            std::vector<int64_t> ap;
+            std::vector<int32_t> adj;
+            ig_status s = ig::fetch_adjacency(g, ap, adj);
+            if (s != IG_OK)
+                return s;
+            *count = ig::greedy_from_adjacency(ap.data(), adj.data(), g->n, order);
+        } else {
+            ig_status s = ig::fetch_host(g);
+            if (s != IG_OK)
+                return s;
+            *count = ig::greedy_from_upper(g->h_row_ptr.data(), g->h_cols.data(), g->n, order_threads, order);
+        }
     } catch (...) {
         return ig::set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
     }

@@ -98,7 +98,7 @@ struct Unit {
     static constexpr bool kTwo = L <= 15;
     static constexpr int kCols = kTwo ? 2 : 1;      // columns per unit
     static constexpr int kVec = kTwo ? 4 : 2;       // uint4 per unit in the stream
-    static constexpr int kUsed = (L + 3) / 4;       // uint4 read per two-lane unit
+    static constexpr int kUsed = kTwo ? (L + 3) / 4 : 2;  // uint4 read per unit
     static constexpr int kBytes = kVec * 16;
     static constexpr int kTileUnits = kTileCols / kCols;
 };
@@ -329,6 +329,7 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
                 emit_hit(a, h1, (uint32_t)row, (uint32_t)(col + 1), seg, rank, lane);
             }
         } else {
+            static_assert(U::kUsed == 2, "one-lane units are two uint4");
             uint32_t sel[8];
             const uint4 q0 = src[0];
             const uint4 q1 = src[1];
@@ -710,6 +711,24 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
 
 }  // namespace
 
+ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m)
+{
+    cudaStream_t st = ctx->stream;
+    const int64_t nb = (m + kScanChunk - 1) / kScanChunk;
+    ig_status s = ensure(ctx, ctx->scan_tmp, (size_t)nb * sizeof(int64_t), "scan workspace");
+    if (s != IG_OK)
+        return s;
+    int64_t *sums = static_cast<int64_t *>(ctx->scan_tmp.ptr);
+    scan_blocks<<<(unsigned)nb, kScanThreads, 0, st>>>(x, m, sums);
+    scan_sums<<<1, kScanThreads, 0, st>>>(sums, nb);
+    scan_add<<<(unsigned)nb, kScanThreads, 0, st>>>(x, m, sums);
+    ctx->launches += 3;
+    IG_CUDA(cudaGetLastError());
+    return IG_OK;
+}
+
+ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what) { return ensure(ctx, b, bytes, what); }
+
 void phase_begin(Ctx *ctx, int phase)
 {
     if (!ctx->profiling)
@@ -841,17 +860,9 @@ ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
     // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
-    const int64_t m = (int64_t)n + 1;
-    const int64_t nb = (m + kScanChunk - 1) / kScanChunk;
-    ig_status s = ensure(ctx, ctx->scan_tmp, (size_t)nb * sizeof(int64_t), "scan workspace");
+    ig_status s = inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1);
     if (s != IG_OK)
         return s;
-    int64_t *sums = static_cast<int64_t *>(ctx->scan_tmp.ptr);
-    scan_blocks<<<(unsigned)nb, kScanThreads, 0, st>>>(g->d_row_ptr, m, sums);
-    scan_sums<<<1, kScanThreads, 0, st>>>(sums, nb);
-    scan_add<<<(unsigned)nb, kScanThreads, 0, st>>>(g->d_row_ptr, m, sums);
-    ctx->launches += 3;
-    IG_CUDA(cudaGetLastError());
     if (total > 0) {
         const int sgrid = (int)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)ctx->sm_count * 16);
         scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), total,

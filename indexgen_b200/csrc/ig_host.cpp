@@ -7,6 +7,7 @@
 // it consumes, as the reference's AdjList does.
 #include <algorithm>
 #include <cstring>
+#include <memory>
 #include <vector>
 
 #include "ig_internal.h"
@@ -41,6 +42,7 @@ void assemble(const int64_t *row_ptr, const int32_t *cols, int32_t n, int T, std
     ap.assign((size_t)n + 1, 0);
     adj.resize((size_t)std::max<int64_t>(2 * nnz, 1));
     std::vector<int32_t> tmp;
+    std::vector<int64_t> rc((size_t)std::max(T, 1) + 1);
     int64_t o = 0;
     for (int32_t x = 0; x < n; ++x) {
         const int32_t *lb = lo.data() + lp[(size_t)x];
@@ -53,12 +55,18 @@ void assemble(const int64_t *row_ptr, const int32_t *cols, int32_t n, int T, std
             std::memcpy(adj.data() + o, ub, (size_t)nu * sizeof(int32_t));
             o += nu;
         } else {
-            tmp.assign(lb, lb + nl);
-            std::stable_sort(tmp.begin(), tmp.end(), [T](int32_t a, int32_t b) { return a % T < b % T; });
+            // stable counting pass by residue w mod T keeps w ascending per group
+            std::fill(rc.begin(), rc.end(), 0);
+            for (int64_t k = 0; k < nl; ++k)
+                rc[(size_t)(lb[k] % T) + 1]++;
+            for (int t = 0; t < T; ++t)
+                rc[(size_t)t + 1] += rc[(size_t)t];
             const int rx = x % T;
-            auto split = std::upper_bound(tmp.begin(), tmp.end(), rx,
-                                          [T](int r, int32_t w) { return r < w % T; });
-            const int64_t head = split - tmp.begin();
+            // upper neighbours follow the lower ones of residue <= x mod T
+            const int64_t head = rc[(size_t)rx + 1];
+            tmp.resize((size_t)nl);
+            for (int64_t k = 0; k < nl; ++k)
+                tmp[(size_t)rc[(size_t)(lb[k] % T)]++] = lb[k];
             std::memcpy(adj.data() + o, tmp.data(), (size_t)head * sizeof(int32_t));
             o += head;
             std::memcpy(adj.data() + o, ub, (size_t)nu * sizeof(int32_t));
@@ -74,25 +82,44 @@ void assemble(const int64_t *row_ptr, const int32_t *cols, int32_t n, int T, std
 // exact semantics of its members (src/SparseMat.cpp:81-266): LIFO buckets,
 // swap-with-last removal, moved rows appended to the lower bucket, and a
 // minimum tracker that only advances when the tracked bucket empties.
+//
+// Layout: the degree doubles as the deletion mark (-1 = deleted; the
+// reference skips deleted neighbours and neighbours of degree 0 alike) and
+// sits next to the bucket position of the same vertex; and
+// all buckets share one flat array: bucket b gets a fixed slice of
+// #{v : initial degree >= b} slots, which bounds its size at any time because
+// degrees only fall.  The slice array is left uninitialised so only the slots
+// actually used are ever touched.
 class BucketGreedy {
   public:
-    BucketGreedy(const int64_t *ap, const int32_t *adj, int32_t n) : ap_(ap), adj_(adj), n_(n)
+    BucketGreedy(const int64_t *ap, const int32_t *adj, int32_t n) : ap_(ap), adj_(adj), v_((size_t)n)
     {
-        deg_.resize((size_t)n);
-        pos_.resize((size_t)n);
-        deleted_.assign((size_t)n, 0);
         int32_t maxd = 0;
         for (int32_t i = 0; i < n; ++i) {
-            deg_[(size_t)i] = (int32_t)(ap[i + 1] - ap[i]);
-            maxd = std::max(maxd, deg_[(size_t)i]);
+            v_[(size_t)i].deg = (int32_t)(ap[i + 1] - ap[i]);
+            maxd = std::max(maxd, v_[(size_t)i].deg);
         }
-        buckets_.resize((size_t)maxd + 1);
+        nb_ = maxd + 1;
+        std::vector<int64_t> hist((size_t)nb_ + 1, 0);
+        for (int32_t i = 0; i < n; ++i)
+            hist[(size_t)v_[(size_t)i].deg]++;
+        // cap_b = #{v : deg >= b}
+        start_.resize((size_t)nb_ + 1);
+        size_.assign((size_t)nb_, 0);
+        int64_t ge = n, off = 0;
+        for (int32_t b = 0; b < nb_; ++b) {
+            start_[(size_t)b] = off;
+            off += ge;
+            ge -= hist[(size_t)b];
+        }
+        start_[(size_t)nb_] = off;
+        data_.reset(new int32_t[(size_t)std::max<int64_t>(off, 1)]);
         tracker_ = maxd + 1;
-        for (int32_t i = 0; i < n; ++i) {  // RowsBySum
-            auto &b = buckets_[(size_t)deg_[(size_t)i]];
-            pos_[(size_t)i] = (int32_t)b.size();
-            b.push_back(i);
-            tracker_ = std::min(tracker_, deg_[(size_t)i]);
+        for (int32_t i = 0; i < n; ++i) {  // RowsBySum: ascending vertex id
+            const int32_t d = v_[(size_t)i].deg;
+            v_[(size_t)i].pos = size_[(size_t)d];
+            data_[(size_t)(start_[(size_t)d] + size_[(size_t)d]++)] = i;
+            tracker_ = std::min(tracker_, d);
         }
         active_ = n;
         todel_.reserve((size_t)maxd + 1);
@@ -102,15 +129,21 @@ class BucketGreedy {
     {
         int32_t cnt = 0;
         while (active_ > 0) {
-            const int32_t x = buckets_[(size_t)tracker_].back();  // MinSumRow
+            // MinSumRow: back of the minimum bucket
+            const int32_t x = data_[(size_t)(start_[(size_t)tracker_] + size_[(size_t)tracker_] - 1)];
             order[cnt++] = x;
-            todel_.clear();  // DelBall
-            for (int64_t k = ap_[x]; k < ap_[x + 1]; ++k)
-                if (!deleted_[(size_t)adj_[k]])
-                    todel_.push_back(adj_[k]);
-            todel_.push_back(x);
-            for (int32_t y : todel_)
-                del_row_col(y);
+            // DelBall: active neighbours in m-order, then the vertex itself
+            const int64_t b = ap_[x], e = ap_[x + 1];
+            todel_.resize((size_t)(e - b) + 1);
+            int32_t nt = 0;
+            for (int64_t k = b; k < e; ++k) {  // branch-free compaction
+                const int32_t j = adj_[k];
+                todel_[(size_t)nt] = j;
+                nt += v_[(size_t)j].deg >= 0;
+            }
+            todel_[(size_t)nt++] = x;
+            for (int32_t t = 0; t < nt; ++t)
+                del_row_col(todel_[(size_t)t]);
         }
         return cnt;
     }
@@ -118,52 +151,72 @@ class BucketGreedy {
   private:
     void delete_row(int32_t cur, int32_t row)
     {
-        auto &b = buckets_[(size_t)cur];
-        const int32_t p = pos_[(size_t)row];
-        const int32_t last = b.back();
-        b[(size_t)p] = last;
-        pos_[(size_t)last] = p;
-        b.pop_back();
-        if (cur == tracker_ && b.empty())
-            while (tracker_ < (int32_t)buckets_.size() && buckets_[(size_t)tracker_].empty())
+        const int64_t base = start_[(size_t)cur];
+        const int32_t sz = --size_[(size_t)cur];
+        const int32_t p = v_[(size_t)row].pos;
+        const int32_t last = data_[(size_t)(base + sz)];
+        data_[(size_t)(base + p)] = last;
+        v_[(size_t)last].pos = p;
+        if (cur == tracker_ && sz == 0)
+            while (tracker_ < nb_ && size_[(size_t)tracker_] == 0)
                 ++tracker_;
     }
 
     void decrease_sum(int32_t cur, int32_t row)
     {
         delete_row(cur, row);
-        deg_[(size_t)row] = cur - 1;
-        auto &b = buckets_[(size_t)cur - 1];
-        pos_[(size_t)row] = (int32_t)b.size();
-        b.push_back(row);
-        if (cur - 1 < tracker_)
-            tracker_ = cur - 1;
+        const int32_t b = cur - 1;
+        const int32_t s = size_[(size_t)b]++;
+        data_[(size_t)(start_[(size_t)b] + s)] = row;
+        v_[(size_t)row].deg = b;
+        v_[(size_t)row].pos = s;
+        if (b < tracker_)
+            tracker_ = b;
     }
 
+    // Neighbours are visited in blocks of 8: their degrees are loaded together
+    // (independent loads overlap) and only the live ones (degree > 0) are
+    // walked through a bitmask.  Exact: within one pass over m[i] the
+    // neighbours are distinct and decrease_sum(j) changes only deg[j].
     void del_row_col(int32_t i)
     {
-        if (deleted_[(size_t)i])
+        const int32_t di = v_[(size_t)i].deg;
+        if (di < 0)
             return;
-        for (int64_t k = ap_[i]; k < ap_[i + 1]; ++k) {
-            const int32_t j = adj_[k];
-            if (deleted_[(size_t)j])
-                continue;
-            const int32_t dj = deg_[(size_t)j];
-            if (dj > 0)
-                decrease_sum(dj, j);
+        const int64_t e = ap_[i + 1];
+        for (int64_t k = ap_[i]; k < e; k += 8) {
+            const int m = (int)std::min<int64_t>(8, e - k);
+            int32_t jj[8], dd[8];
+            unsigned live = 0;
+            for (int t = 0; t < m; ++t) {
+                jj[t] = adj_[k + t];
+                dd[t] = v_[(size_t)jj[t]].deg;
+            }
+            for (int t = 0; t < m; ++t)
+                live |= (unsigned)(dd[t] > 0) << t;
+            while (live) {
+                const int t = __builtin_ctz(live);
+                live &= live - 1;
+                decrease_sum(dd[t], jj[t]);
+            }
         }
-        delete_row(deg_[(size_t)i], i);
-        deleted_[(size_t)i] = 1;
+        delete_row(v_[(size_t)i].deg, i);
+        v_[(size_t)i].deg = -1;
         --active_;
     }
 
+    struct Vtx {
+        int32_t deg;  // current degree, -1 once deleted
+        int32_t pos;  // slot inside its degree bucket
+    };
     const int64_t *ap_;
     const int32_t *adj_;
-    int32_t n_;
-    std::vector<int32_t> deg_, pos_;
-    std::vector<uint8_t> deleted_;
-    std::vector<std::vector<int32_t>> buckets_;
+    std::vector<Vtx> v_;
+    std::vector<int32_t> size_;
+    std::vector<int64_t> start_;
+    std::unique_ptr<int32_t[]> data_;
     std::vector<int32_t> todel_;
+    int32_t nb_ = 0;
     int32_t tracker_ = 0;
     int32_t active_ = 0;
 };
@@ -179,6 +232,14 @@ int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n
     std::vector<int32_t> adj;
     assemble(row_ptr, cols, n, order_threads, ap, adj);
     BucketGreedy g(ap.data(), adj.data(), n);
+    return g.run(order);
+}
+
+int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order)
+{
+    if (n <= 0)
+        return 0;
+    BucketGreedy g(adj_ptr, adj, n);
     return g.run(order);
 }
 

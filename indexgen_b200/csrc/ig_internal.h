@@ -36,7 +36,7 @@ struct Ctx {
     std::string last_error;
     int64_t launches = 0;
     // workspace
-    DevBuf words, sel, counts, records, scan_tmp, flags;
+    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp;
     unsigned long long rec_capacity = 0;  // records that fit in `records`
     // optional per-phase timing (IG_PHASE_*)
     bool profiling = false;
@@ -63,6 +63,9 @@ struct Graph {
     std::vector<int64_t> h_row_ptr;
     std::vector<int32_t> h_cols;
     bool host_valid = false;
+    // symmetric adjacency in canonical order (built on first request)
+    int64_t *d_adj_ptr = nullptr;  // [n+1]
+    int32_t *d_adj = nullptr;      // [2*edges]
 };
 
 // Geometry of the upper-triangle work decomposition for one job.
@@ -81,9 +84,17 @@ PairPlan make_plan(int32_t n, int grid_ctas);
 ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, Graph *g);
 ig_status count_edges(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, int64_t *edges);
 
+// In-place inclusive scan of m int64 on the context stream (ig_graph.cu).
+ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m);
+ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what);
+// Symmetric CSR in the canonical neighbour order (ig_adjacency.cu).
+ig_status build_adjacency(Ctx *ctx, Graph *g);
+
 // Host greedy (ig_host.cpp).
 int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                           int32_t *order);
+// Greedy directly over neighbour lists already in m-order.
+int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order);
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);

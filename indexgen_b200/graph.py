@@ -128,6 +128,14 @@ class ConflictGraph:
         check(lib().ig_graph_device_csr(self.handle, ctypes.byref(rp), ctypes.byref(cl)), "ig_graph_device_csr")
         return int(rp.value or 0), int(cl.value or 0)
 
+    def adjacency(self):
+        """Symmetric neighbour lists in the canonical (sorted) order, as CSR."""
+        adj_ptr = np.zeros(self.n + 1, np.int64)
+        adj = np.zeros(2 * self.edges, np.int32)
+        check(lib().ig_graph_adjacency(self.handle, ptr(adj_ptr), ptr(adj)), "ig_graph_adjacency",
+              self.ctx.handle)
+        return adj_ptr, adj
+
     def codebook(self, order_threads: int = 1) -> np.ndarray:
         order = np.zeros(max(self.n, 1), np.int32)
         cnt = ctypes.c_int32()
@@ -137,14 +145,9 @@ class ConflictGraph:
 
     def adj_list(self):
         """Neighbour lists in both directions, ascending (list of lists)."""
-        row_ptr, cols = self.upper_csr()
-        adj = [[] for _ in range(self.n)]
-        rows = np.repeat(np.arange(self.n), np.diff(row_ptr))
-        for u, v in zip(rows.tolist(), cols.tolist()):
-            adj[v].append(u)
-        for u in range(self.n):
-            adj[u].extend(cols[row_ptr[u]:row_ptr[u + 1]].tolist())
-        return adj
+        adj_ptr, adj = self.adjacency()
+        flat = adj.tolist()
+        return [flat[adj_ptr[u]:adj_ptr[u + 1]] for u in range(self.n)]
 
     def close(self):
         if self.handle:

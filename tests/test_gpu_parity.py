@@ -206,3 +206,47 @@ def test_repeated_builds_are_identical(igctx):
             ref = r
         else:
             assert np.array_equal(ref[0], r[0]) and np.array_equal(ref[1], r[1])
+
+
+def test_adjacency_matches_oracle_order(igctx, oracle):
+    """Device-built symmetric lists equal the reference loader's order (T=1)."""
+    from indexgen_b200 import build_conflict_graph
+
+    g = load_golden("small_cases.npz")
+    cases = [(g[k + "_words"], int(k.split("_")[0][1:]), int(k.split("_")[1][1:])) for k in
+             sorted({k.rsplit("_", 1)[0] for k in g.files if k.endswith("_words")})]
+    u = load_golden("uniform11.npz")
+    cases.append((u["words"], 11, 3))
+    for w, L, d in cases:
+        rp, cols = oracle.conflict_upper(w, L, d)
+        ap_o, adj_o = oracle.adjacency(rp, cols, len(w), 1)
+        with build_conflict_graph(w, L, d, igctx) as G:
+            ap, adj = G.adjacency()
+        assert np.array_equal(ap, ap_o) and np.array_equal(adj, adj_o), (L, d)
+
+
+def test_adjacency_long_rows(igctx):
+    """Rows with more than 1024 lower neighbours take the bitmap path; the last
+    row's neighbours span two 512 Ki-value bitmap windows."""
+    from indexgen_b200 import build_conflict_graph, workloads as W
+
+    n = 530_000
+    w = W.uniform_words(n, 16, 1234)
+    clique = np.r_[np.arange(1100), n - 1]
+    w[clique] = w[0]
+    with build_conflict_graph(w, 16, 1, igctx) as G:
+        ap, adj = G.adjacency()
+        rp, cols = G.upper_csr()
+    _, counts = np.unique(w, return_counts=True)
+    assert G.edges == int((counts * (counts - 1) // 2).sum())  # editDist 1: exact duplicates
+    last = adj[ap[n - 1]:ap[n]]
+    assert last.tolist() == np.nonzero(w[: n - 1] == w[n - 1])[0].tolist()
+    assert len(last) >= 1100
+    # every row: lower part ascending and < x, upper part equals the CSR row
+    deg_up = np.diff(rp)
+    deg = np.diff(ap)
+    for x in (0, 1, 500, 1099):
+        row = adj[ap[x]:ap[x + 1]]
+        lo, up = row[: deg[x] - deg_up[x]], row[deg[x] - deg_up[x]:]
+        assert np.all(np.diff(lo) > 0) and np.all(lo < x)
+        assert np.array_equal(up, cols[rp[x]:rp[x + 1]])
