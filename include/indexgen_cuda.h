@@ -132,6 +132,25 @@ ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int 
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count);
 
+/* ---- allocation-free variant ------------------------------------------- */
+
+/* No counterpart in the reference.  Counts the pairs i<j with ED < min_ed
+ * like ig_count_conflicts, but never allocates device memory: for hosts that
+ * manage every device byte themselves (a fixed arena handed out by a JVM, Go
+ * or Rust runtime, a hard per-process memory budget) or that must not enter
+ * the allocator where it could block or fail.  `words` (n packed words) and
+ * `count` (one unsigned 64-bit integer) are device pointers owned by the
+ * caller; the work is queued on `stream` (a cudaStream_t; NULL = the default
+ * stream) of the current device and the call returns without waiting.  The
+ * scratch is a fixed array inside the library image, at most
+ * IG_NOALLOC_MAX_WORDS words per call (larger n: IG_ERR_CAPACITY).  The first
+ * call on each device looks up that array's device address; make it before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+#define IG_NOALLOC_MAX_WORDS 65536
+ig_status ig_count_conflicts_noalloc(const uint32_t *words, int32_t n, int len, int min_ed,
+                                     unsigned long long *count, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,7 +19,7 @@ EXPORTS = (
     "ig_ctx_reserve", "ig_ctx_launches", "ig_ctx_set_profiling", "ig_ctx_phase_time", "ig_pack", "ig_filter", "ig_graph_build", "ig_graph_free",
     "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_adjacency",
     "ig_graph_device_adjacency", "ig_graph_codebook",
-    "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr",
+    "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -67,6 +67,7 @@ def _declare(L):
         "ig_solve": (_int, [_vp, _vp, _i32, _int, _int, _int, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
         "ig_count_conflicts": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),
         "ig_codebook_from_upper_csr": (_int, [_vp, _vp, _i32, _int, _vp, ctypes.POINTER(_i32)]),
+        "ig_count_conflicts_noalloc": (_int, [_vp, _i32, _int, _int, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
