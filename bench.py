@@ -222,6 +222,47 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
+def run_batch_section(ctx, reps: int = 3) -> dict:
+    """Batched clusters (1,000,000 filtered uniform n=14 words, 64 clusters with
+    Zipf(1.1) sizes in [2k, 60k], editDist 4): the whole batch as one device
+    pipeline + per-cluster greedies on all host cores, against the plain path
+    that solves the clusters one after another (one graph build + one greedy
+    per cluster).  Both through the public API with host buffers."""
+    from indexgen_b200 import solve, solve_batch
+
+    parts = W.clustered14()
+    jobs = [(w, 14, 4) for w in parts]
+    pairs = sum(len(w) * (len(w) - 1) // 2 for w in parts)
+    cores = host_cores()
+    books, edges = solve_batch(jobs, host_threads=cores, ctx=ctx)  # warm-up (workspace growth)
+    ctx.set_profiling(True)
+    t_batch = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        books, edges = solve_batch(jobs, host_threads=cores, ctx=ctx)
+        t_batch.append(time.perf_counter() - t0)
+    pair_ms, pair_launches = ctx.phase_time(0)
+    ctx.set_profiling(False)
+    solve(jobs[0][0], 14, 4, 1, ctx)  # warm-up
+    t0 = time.perf_counter()
+    plain_books = []
+    for w, L, d in jobs:
+        plain_books.append(solve(w, L, d, 1, ctx)[0])
+    t_plain = time.perf_counter() - t0
+    same = all(np.array_equal(a, b) for a, b in zip(books, plain_books))
+    tb = min(t_batch)
+    return {"workload": "clusters64_n14_d4 (1,000,000 uniform n=14 words, 64 Zipf(1.1) clusters in [2k,60k])",
+            "jobs": len(jobs), "pair_tests": pairs, "edges": int(np.sum(edges)),
+            "codebook_words": int(sum(len(b) for b in books)),
+            "batched_jobs_per_s": len(jobs) / tb, "batched_s": tb,
+            "plain_jobs_per_s": len(jobs) / t_plain, "plain_s": t_plain,
+            "speedup_vs_plain": t_plain / tb,
+            "batched_pair_kernel_gpairs_per_s": (pairs / (pair_ms / pair_launches / 1e3) / 1e9)
+            if pair_launches else None,
+            "host_threads": cores, "identical_to_plain": bool(same),
+            "note": "wall clock through solve_batch vs a loop of solve (graph + greedy per cluster)"}
+
+
 def run_ours(args, wl, rank, world, dist):
     import ctypes
 
@@ -350,6 +391,8 @@ def run_ours(args, wl, rank, world, dist):
         "clocks": clk,
         "greedy": {"ms": greedy_ms, "codebook": int(len(sel)), "order_threads": 1, "where": "host C++ (library)"},
     }
+    if not args.no_batch:
+        line["batch"] = run_batch_section(ctx)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)
     if rank == 0:
@@ -365,6 +408,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-clusters section")
     ap.add_argument("--subset", type=int, default=0,
                     help="use a seeded random subset of this many words (profiling runs)")
     args = ap.parse_args()

@@ -112,12 +112,34 @@ ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const 
 ig_status ig_graph_adjacency(ig_graph *g, int64_t *adj_ptr, int32_t *adj);
 /* Device pointers of that adjacency (built on first request). */
 ig_status ig_graph_device_adjacency(ig_graph *g, const int64_t **adj_ptr, const int32_t **adj);
-/* Greedy minimum-degree independent set over the graph, reproducing AdjList's
+/* Greedy minimum-degree independent set over a single-job graph, reproducing AdjList's
  * selection order (src/SparseMat.cpp:81-266, :679-731) for neighbour lists
  * assembled as FillAdjList(order_threads) does (src/SparseMat.cpp:599-609);
  * order_threads = 1 is the sorted order the GPU-path loader builds.
  * order[] receives up to n vertex ids in selection order; *count their number. */
 ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int32_t *count);
+
+/* ---- batches of independent jobs --------------------------------------- */
+/* The clustered solve runs SolveIndependentSet once per cluster from a pool of
+ * host threads (src/SparseMat.cpp:927-1095, :784-851), one python3 process
+ * per cluster on the GPU path.  Here a whole batch of jobs is one device
+ * pipeline with ONE persistent pair-test launch; job j is words
+ * [offsets[j], offsets[j+1]) of length lens[j] with threshold min_eds[j].
+ * The result is one graph whose CSR is block diagonal over the jobs (global
+ * word ids); jobs never share an edge. */
+ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
+                         const int32_t *lens, const int32_t *min_eds, int words_on_device, ig_graph **out);
+ig_status ig_graph_job_count(const ig_graph *g, int32_t *jobs);
+ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word, int32_t *n, int64_t *edges);
+/* Greedy of every job on host_threads host threads (0 = all cores), largest
+ * job first.  Job j's codebook, as job-local vertex ids in selection order,
+ * is written to order + offsets[j]; counts[j] is its size.  order_threads as
+ * in ig_graph_codebook. */
+ig_status ig_graph_job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts);
+/* Build + job codebooks in one call; edges[j] (optional) = edges of job j. */
+ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
+                         const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
+                         int32_t *order, int32_t *counts, int64_t *edges);
 
 /* ---- one-call conveniences --------------------------------------------- */
 

@@ -10,6 +10,7 @@ from .graph import (  # noqa: F401
     Context,
     IndexGenError,
     apply_filters,
+    build_batch,
     build_conflict_graph,
     codebook_from_upper_csr,
     count_conflicts,
@@ -17,6 +18,7 @@ from .graph import (  # noqa: F401
     fill_adj_list_gpu,
     pack_sequences,
     solve,
+    solve_batch,
     solve_edit_distance_cuda,
     solve_independent_set,
     verify_dist,

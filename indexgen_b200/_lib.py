@@ -20,6 +20,7 @@ EXPORTS = (
     "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_adjacency",
     "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
+    "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_codebooks", "ig_solve_batch",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -68,6 +69,11 @@ def _declare(L):
         "ig_count_conflicts": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),
         "ig_codebook_from_upper_csr": (_int, [_vp, _vp, _i32, _int, _vp, ctypes.POINTER(_i32)]),
         "ig_count_conflicts_noalloc": (_int, [_vp, _i32, _int, _int, _vp, _vp]),
+        "ig_batch_build": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, ctypes.POINTER(_vp)]),
+        "ig_graph_job_count": (_int, [_vp, ctypes.POINTER(_i32)]),
+        "ig_graph_job_stats": (_int, [_vp, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
+        "ig_graph_job_codebooks": (_int, [_vp, _int, _int, _vp, _vp]),
+        "ig_solve_batch": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, _int, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

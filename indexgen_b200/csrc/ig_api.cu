@@ -1,9 +1,12 @@
 // C ABI of libindexgen_cuda (declarations and reference citations in
 // include/indexgen_cuda.h).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
+#include <numeric>
 #include <string>
+#include <thread>
 
 #include "ig_internal.h"
 
@@ -148,6 +151,80 @@ ig_status fetch_adjacency(ig_graph *g, std::vector<int64_t> &ap, std::vector<int
         e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess)
         return cuda_error(ctx, e, "adjacency download");
+    return IG_OK;
+}
+
+// Greedy of every job of a graph on `host_threads` host threads, largest job
+// first.  Job j's selection (job-local ids) goes to order + word_off_j.
+ig_status job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
+{
+    std::vector<int64_t> ap;
+    std::vector<int32_t> adj;
+    ig_status s = order_threads == 1 ? fetch_adjacency(g, ap, adj) : fetch_host(g);
+    if (s != IG_OK)
+        return s;
+    const int k = (int)g->jobs.size();
+    std::vector<int> seq((size_t)k);
+    std::iota(seq.begin(), seq.end(), 0);
+    std::stable_sort(seq.begin(), seq.end(), [&](int a, int b) {
+        return g->job_edge_off[(size_t)a + 1] - g->job_edge_off[(size_t)a] >
+               g->job_edge_off[(size_t)b + 1] - g->job_edge_off[(size_t)b];
+    });
+    std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
+    auto worker = [&]() {
+        for (;;) {
+            const int q = next++;
+            if (q >= k)
+                return;
+            const JobSpec &J = g->jobs[(size_t)seq[(size_t)q]];
+            try {
+                int32_t c;
+                if (order_threads == 1)
+                    c = greedy_from_adjacency(ap.data() + J.word_off, adj.data(), J.n, J.word_off,
+                                              order + J.word_off);
+                else
+                    c = greedy_from_upper(g->h_row_ptr.data() + J.word_off, g->h_cols.data(), J.n, J.word_off,
+                                          order_threads, order + J.word_off);
+                counts[seq[(size_t)q]] = c;
+            } catch (...) {
+                failed = true;
+            }
+        }
+    };
+    int T = host_threads > 0 ? host_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    T = std::max(1, std::min(T, k));
+    if (T == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; ++t)
+            pool.emplace_back(worker);
+        for (auto &th : pool)
+            th.join();
+    }
+    if (failed)
+        return set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
+    return IG_OK;
+}
+
+// Validated job list from an offsets array.
+ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *lens, const int32_t *min_eds,
+                    std::vector<JobSpec> &jobs)
+{
+    if (k < 0 || (k > 0 && (!offsets || !lens || !min_eds)))
+        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[k+1], lens[k] and min_eds[k] are required");
+    if (k > 0 && offsets[0] != 0)
+        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[0] must be 0");
+    jobs.clear();
+    for (int32_t j = 0; j < k; ++j) {
+        const int64_t n = offsets[j + 1] - offsets[j];
+        if (n < 0 || n > INT32_MAX || lens[j] < 1 || lens[j] > IG_MAX_LEN)
+            return set_error(ctx, IG_ERR_INPUT, "jobs: offsets must not decrease and 1 <= len <= 16");
+        jobs.push_back(JobSpec{offsets[j], (int32_t)n, lens[j], min_eds[j]});
+    }
+    if (k > 0 && offsets[k] > INT32_MAX)
+        return set_error(ctx, IG_ERR_CAPACITY, "more than 2^31-1 words in one batch");
     return IG_OK;
 }
 
@@ -312,7 +389,7 @@ ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len,
     const uint32_t *d_words = nullptr;
     ig_status s = ig::stage_words(ctx, words, n, words_on_device, &d_words);
     if (s == IG_OK)
-        s = ig::build_graph(ctx, d_words, n, len, min_ed, g);
+        s = ig::build_batch(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, g);
     if (s != IG_OK) {
         ig::release_graph(g);
         return s;
@@ -434,25 +511,91 @@ ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int3
 {
     if (!g || !count || order_threads < 1 || (g->n > 0 && !order))
         return IG_ERR_INPUT;
-    try {
-        if (order_threads == 1) {
-            // canonical order: lists come ready from the device
-            std::vector<int64_t> ap;
-            std::vector<int32_t> adj;
-            ig_status s = ig::fetch_adjacency(g, ap, adj);
-            if (s != IG_OK)
-                return s;
-            *count = ig::greedy_from_adjacency(ap.data(), adj.data(), g->n, order);
-        } else {
-            ig_status s = ig::fetch_host(g);
-            if (s != IG_OK)
-                return s;
-            *count = ig::greedy_from_upper(g->h_row_ptr.data(), g->h_cols.data(), g->n, order_threads, order);
-        }
-    } catch (...) {
-        return ig::set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
-    }
+    if (g->jobs.size() != 1)
+        return ig::set_error(g->ctx, IG_ERR_STATE, "graph holds several jobs: use ig_graph_job_codebooks");
+    int32_t c = 0;
+    ig_status s = ig::job_codebooks(g, order_threads, 1, order, &c);
+    if (s == IG_OK)
+        *count = c;
+    return s;
+}
+
+ig_status ig_graph_job_count(const ig_graph *g, int32_t *jobs)
+{
+    if (!g || !jobs)
+        return IG_ERR_INPUT;
+    *jobs = (int32_t)g->jobs.size();
     return IG_OK;
+}
+
+ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word, int32_t *n, int64_t *edges)
+{
+    if (!g || job < 0 || job >= (int32_t)g->jobs.size())
+        return IG_ERR_INPUT;
+    if (first_word)
+        *first_word = g->jobs[(size_t)job].word_off;
+    if (n)
+        *n = g->jobs[(size_t)job].n;
+    if (edges)
+        *edges = g->job_edge_off[(size_t)job + 1] - g->job_edge_off[(size_t)job];
+    return IG_OK;
+}
+
+ig_status ig_graph_job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
+{
+    if (!g || order_threads < 1 || (g->n > 0 && !order) || (!g->jobs.empty() && !counts))
+        return IG_ERR_INPUT;
+    return ig::job_codebooks(g, order_threads, host_threads, order, counts);
+}
+
+ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
+                         const int32_t *lens, const int32_t *min_eds, int words_on_device, ig_graph **out)
+{
+    if (!ctx || !out)
+        return IG_ERR_INPUT;
+    *out = nullptr;
+    std::vector<ig::JobSpec> spec;
+    ig_status s = ig::make_jobs(ctx, offsets, jobs, lens, min_eds, spec);
+    if (s != IG_OK)
+        return s;
+    const int64_t total = jobs > 0 ? offsets[jobs] : 0;
+    if (total > 0 && !words)
+        return ig::set_error(ctx, IG_ERR_INPUT, "words must be non-null");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    ig_graph *g = new (std::nothrow) ig_graph();
+    if (!g)
+        return IG_ERR_OOM;
+    const uint32_t *d_words = nullptr;
+    s = ig::stage_words(ctx, words, (int32_t)total, words_on_device, &d_words);
+    if (s == IG_OK)
+        s = ig::build_batch(ctx, d_words, spec, g);
+    if (s != IG_OK) {
+        ig::release_graph(g);
+        return s;
+    }
+    *out = g;
+    return IG_OK;
+}
+
+ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
+                         const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
+                         int32_t *order, int32_t *counts, int64_t *edges)
+{
+    if (!ctx || order_threads < 1 || (jobs > 0 && (!order || !counts)))
+        return IG_ERR_INPUT;
+    ig_graph *g = nullptr;
+    ig_status s = ig_batch_build(ctx, words, offsets, jobs, lens, min_eds, 0, &g);
+    if (s != IG_OK)
+        return s;
+    if (edges)
+        for (int32_t j = 0; j < jobs; ++j)
+            edges[j] = g->job_edge_off[(size_t)j + 1] - g->job_edge_off[(size_t)j];
+    s = ig::job_codebooks(g, order_threads, host_threads, order, counts);
+    ig::release_graph(g);
+    return s;
 }
 
 ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,
@@ -483,7 +626,7 @@ ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int 
     ig_status s = ig::stage_words(ctx, words, n, 0, &d_words);
     if (s != IG_OK)
         return s;
-    return ig::count_edges(ctx, d_words, n, len, min_ed, edges);
+    return ig::count_batch(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, edges);
 }
 
 }  // extern "C"

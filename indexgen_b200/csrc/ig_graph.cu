@@ -3,23 +3,27 @@
 // Replaces compute_chunk_kernel + the tile loop of src/cuda_edit_distance.py
 // (:20-226, :278-446) and the Python edge writer (src/gpu_graph_generator.py:49-77).
 //
-// Pipeline for one job of n words of length L and threshold d (edge iff ED < d):
+// Pipeline for a batch of independent jobs (one job = n words of one length L
+// and a threshold d; edge iff ED < d).  A single job is a batch of one; the
+// clustered solve (src/SparseMat.cpp:927-1095) submits all clusters at once.
 //   prep_units      words -> PRMT selector streams, two columns per unit for L <= 15
-//   pair_kernel<L>  persistent CTAs take (row band, column segment) items from an
-//                   atomic queue; 256 rows per band live in registers as two PRMT
+//   pair_kernel     ONE persistent launch for the whole batch: CTAs take
+//                   (job, row band, column segment) items from an atomic queue and
+//                   dispatch on the job's L; 256 rows per band live in registers as two PRMT
 //                   pools of Myers Peq masks; column tiles of the segment are
 //                   staged into shared memory by cp.async.bulk (TMA bulk copy, no
 //                   multicast) with a two-slot mbarrier pipeline; each thread runs
 //                   the 32-bit Myers recurrence on two columns at once (two
 //                   16-bit lanes, L <= 15) or one (L = 16) and emits hits
 //                   through warp ballot + one atomic per warp as
-//                   (row, col, rank-in-(row,segment), segment) records, plus a
+//                   (row, col, rank-in-(row,segment), cell) records, plus a
 //                   per-(row, segment) count.
 //   row_prefix      per-row exclusive prefix over its segments + degree
 //   scan            exclusive scan of degrees -> row_ptr (int64)
-//   scatter         cols[row_ptr[r] + prefix[s][r] + rank] = col
-// The result is the upper CSR with ascending columns, bit-exact by construction
-// (no sort, no order dependence on scheduling).
+//   scatter         cols[row_ptr[r] + prefix[cell] + rank] = col
+// The result is one upper CSR over the concatenated rows with global column
+// ids (block diagonal: jobs never share an edge), ascending per row and
+// bit-exact by construction (no sort, no dependence on scheduling).
 #include <algorithm>
 #include <cstdio>
 
@@ -89,72 +93,98 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
-// units of two columns (L <= 15): out[4*p .. 4*p+3] for columns 2p, 2p+1
-__global__ void prep_units2(const uint32_t *__restrict__ words, int32_t n, int len, uint4 *__restrict__ out)
+// Index of the job whose `key` range contains v (jobs sorted by key).
+__device__ __forceinline__ int find_job_by_item(const JobDesc *jobs, int njobs, long long v)
 {
-    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (p >= ((int64_t)n + 1) / 2)
-        return;
-    const uint32_t wa = words[2 * p];
-    const uint32_t wb = (2 * p + 1 < n) ? words[2 * p + 1] : wa;
-    uint32_t o[16];
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        o[k] = 0u;
-        if (k < len)
-            o[k] = nib((wa >> (2 * k)) & 3u) | (nib((wb >> (2 * k)) & 3u) << 8);
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].item_off <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
     }
-    uint4 *dst = out + 4 * p;
-    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
-    dst[2] = make_uint4(o[8], o[9], o[10], o[11]);
-    dst[3] = make_uint4(o[12], o[13], o[14], o[15]);
+    return lo;
 }
 
-// units of one column (L = 16): out[2*i .. 2*i+1], two positions per word
-__global__ void prep_units1(const uint32_t *__restrict__ words, int32_t n, int len, uint4 *__restrict__ out)
+__device__ __forceinline__ int find_job_by_unit(const JobDesc *jobs, int njobs, long long v)
 {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    const uint32_t w = words[i];
-    uint32_t o[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        o[j] = 0u;
-        if (2 * j < len)
-            o[j] |= nib((w >> (4 * j)) & 3u);
-        if (2 * j + 1 < len)
-            o[j] |= nib((w >> (4 * j + 2)) & 3u) << 16;
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].unit_start <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
     }
-    uint4 *dst = out + 2 * i;
-    dst[0] = make_uint4(o[0], o[1], o[2], o[3]);
-    dst[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    return lo;
+}
+
+__device__ __forceinline__ int find_job_by_row(const JobDesc *jobs, int njobs, long long v)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].word_off <= v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Column units of every job: two columns per unit (16 selector words) for
+// L <= 15, one column per unit (8 words, two positions each) for L = 16.
+__global__ void prep_units(const uint32_t *__restrict__ words, const JobDesc *__restrict__ jobs, int njobs,
+                           long long total_units, uint4 *__restrict__ units)
+{
+    const long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (u >= total_units)
+        return;
+    const JobDesc J = jobs[find_job_by_unit(jobs, njobs, u)];
+    const long long p = u - J.unit_start;
+    const uint32_t *w = words + J.word_off;
+    uint4 *out = units + J.unit_off;
+    if (J.L <= 15) {
+        const uint32_t wa = w[2 * p];
+        const uint32_t wb = (2 * p + 1 < J.n) ? w[2 * p + 1] : wa;
+        uint32_t o[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            o[k] = (k < J.L) ? (nib((wa >> (2 * k)) & 3u) | (nib((wb >> (2 * k)) & 3u) << 8)) : 0u;
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            out[4 * p + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+    } else {
+        const uint32_t x = w[p];
+        uint32_t o[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            o[j] = nib((x >> (4 * j)) & 3u) | (nib((x >> (4 * j + 2)) & 3u) << 16);
+        out[2 * p] = make_uint4(o[0], o[1], o[2], o[3]);
+        out[2 * p + 1] = make_uint4(o[4], o[5], o[6], o[7]);
+    }
 }
 
 struct PairArgs {
     const uint4 *units;
     const uint32_t *words;
-    int32_t n;
-    int lim;          // min_ed - L: a pair is an edge iff popc(Pv) - popc(Mv) < lim
+    const JobDesc *jobs;
+    int njobs;
+    long long items;
     uint32_t one;     // 1 and 2 (and 1 << 16) as opaque operands for imad / umulhi
     uint32_t two;
     uint32_t hi;
-    int seg_shift;
-    int nseg;
-    int bands_per_seg;
-    int nbands;
-    long long items;
     unsigned long long *work;
     unsigned long long *rec_count;
     EdgeRecord *rec;
     unsigned long long rec_cap;
-    uint32_t *counts;  // [nseg][n]
+    uint32_t *counts;
     int *status;
     int emit;
 };
 
-__device__ __forceinline__ void emit_hit(const PairArgs &a, bool hit, uint32_t row, uint32_t col, uint32_t seg,
+__device__ __forceinline__ void emit_hit(const PairArgs &a, bool hit, uint32_t row, uint32_t col, uint32_t cell,
                                          uint32_t &rank, int lane)
 {
     const unsigned m = __ballot_sync(kFull, hit);
@@ -172,20 +202,31 @@ __device__ __forceinline__ void emit_hit(const PairArgs &a, bool hit, uint32_t r
             r.row = row;
             r.col = col;
             r.rank = rank;
-            r.seg = seg;
+            r.cell = cell;
             *reinterpret_cast<uint4 *>(a.rec + idx) = *reinterpret_cast<const uint4 *>(&r);
         }
         ++rank;
     }
 }
 
-// One staged tile of nu units whose first column is c0.  CHECK adds the
-// strict-upper-triangle test (col > row), row < n and col < n; it is only
-// needed on diagonal items, the last (partial) band and an odd last column.
+// Everything one thread needs about its row while it walks a segment.
+struct RowCtx {
+    int32_t row;     // job-local row
+    bool ok;         // row < n
+    uint32_t p01, p23;
+    uint32_t grow;   // global row
+    uint32_t base;   // global id of the job's column 0
+    uint32_t cell;   // index of this (row, segment) count
+    int32_t n;
+    int lim;
+};
+
+// One staged tile of nu units whose first (job-local) column is c0.  CHECK
+// adds the strict-upper-triangle test (col > row), row < n and col < n; it is
+// only needed on diagonal items, the last (partial) band and an odd last column.
 template <int L, bool CHECK>
-__device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, int nu, int32_t c0, int32_t row,
-                                          bool row_ok, uint32_t p01, uint32_t p23, uint32_t seg, uint32_t &rank,
-                                          int lane)
+__device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, int nu, int32_t c0, const RowCtx &r,
+                                          uint32_t &rank, int lane)
 {
     using U = Unit<L>;
     for (int u = 0; u < nu; ++u) {
@@ -205,15 +246,15 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
                 }
             }
             bool h0, h1;
-            myers_two<L>(p01, p23, sel, a.one, a.two, a.lim, h0, h1);
+            myers_two<L>(r.p01, r.p23, sel, a.one, a.two, r.lim, h0, h1);
             const int32_t col = c0 + 2 * u;
             if (CHECK) {
-                h0 = h0 && row_ok && (col > row) && (col < a.n);
-                h1 = h1 && row_ok && (col + 1 > row) && (col + 1 < a.n);
+                h0 = h0 && r.ok && (col > r.row) && (col < r.n);
+                h1 = h1 && r.ok && (col + 1 > r.row) && (col + 1 < r.n);
             }
             if (__any_sync(kFull, h0 || h1)) {
-                emit_hit(a, h0, (uint32_t)row, (uint32_t)col, seg, rank, lane);
-                emit_hit(a, h1, (uint32_t)row, (uint32_t)(col + 1), seg, rank, lane);
+                emit_hit(a, h0, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
+                emit_hit(a, h1, r.grow, r.base + (uint32_t)(col + 1), r.cell, rank, lane);
             }
         } else {
             static_assert(U::kUsed == 2, "one-lane units are two uint4");
@@ -222,26 +263,108 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
             const uint4 q1 = src[1];
             sel[0] = q0.x; sel[1] = q0.y; sel[2] = q0.z; sel[3] = q0.w;
             sel[4] = q1.x; sel[5] = q1.y; sel[6] = q1.z; sel[7] = q1.w;
-            bool h0 = myers_one<L>(p01, p23, sel, a.one, a.two, a.hi, a.lim);
+            bool h0 = myers_one<L>(r.p01, r.p23, sel, a.one, a.two, a.hi, r.lim);
             const int32_t col = c0 + u;
             if (CHECK)
-                h0 = h0 && row_ok && (col > row);
+                h0 = h0 && r.ok && (col > r.row);
             if (__any_sync(kFull, h0))
-                emit_hit(a, h0, (uint32_t)row, (uint32_t)col, seg, rank, lane);
+                emit_hit(a, h0, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
         }
     }
 }
 
+constexpr int kSlotVec = kTileCols * 2;  // uint4 per staged tile (8 KiB, both unit layouts)
+
+// One (band, segment) item of job J: stream the segment's column tiles through
+// the two-slot ring and test them against the band's rows.
 template <int L>
-__global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
+__device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, int band, int seg,
+                                         uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity, bool &aborted)
 {
     using U = Unit<L>;
-    __shared__ __align__(128) uint4 tile[2][U::kTileUnits * U::kVec];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int32_t row0 = band * kBandRows;
+    RowCtx r;
+    r.row = row0 + tid;
+    r.ok = r.row < J.n;
+    r.n = J.n;
+    r.lim = J.lim;
+    r.base = (uint32_t)J.word_off;
+    r.grow = (uint32_t)(J.word_off + r.row);
+    r.cell = (uint32_t)(J.count_off + (long long)seg * J.n + r.row);
+    row_pools<L>(a.words[J.word_off + (r.ok ? r.row : 0)], r.p01, r.p23);
+    // c_lo is a multiple of 256 (segments and bands are), so units never
+    // straddle a segment
+    const int32_t c_lo = (int32_t)max((long long)seg << J.seg_shift, (long long)row0);
+    const int32_t c_hi = (int32_t)min((long long)(seg + 1) << J.seg_shift, (long long)J.n);
+    const long long row_end = (long long)row0 + kBandRows;
+    const bool check = ((long long)c_lo < row_end) || (row_end > (long long)J.n) || (U::kCols == 2 && (c_hi & 1));
+    const int ntiles = (c_hi - c_lo + kTileCols - 1) / kTileCols;
+    const uint4 *units = a.units + J.unit_off;
+    uint32_t rank = 0;
+
+    if (tid == 0) {
+        for (int t = 0; t < 2 && t < ntiles; ++t) {
+            const int32_t c0 = c_lo + t * kTileCols;
+            const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
+            const uint32_t bytes = (uint32_t)nu * U::kBytes;
+            mbar_arrive_expect_tx(&bar[t], bytes);
+            bulk_g2s(&tile[t][0], units + (size_t)(c0 / U::kCols) * U::kVec, bytes, &bar[t]);
+        }
+    }
+    for (int t = 0; t < ntiles; ++t) {
+        const int b = t & 1;
+        bool timed_out = false;
+        const long long t_start = clock64();
+        while (!mbar_try_wait(&bar[b], (parity >> b) & 1u)) {
+            if (clock64() - t_start > kMaxWaitCycles) {
+                timed_out = true;
+                break;
+            }
+        }
+        parity ^= 1u << b;
+        // uniform decision: every thread leaves together if any gave up
+        if (__syncthreads_or(timed_out)) {
+            if (tid == 0)
+                atomicExch(a.status, kStatusTimeout);
+            aborted = true;
+            return;
+        }
+        const int32_t c0 = c_lo + t * kTileCols;
+        const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
+        if (check)
+            tile_pass<L, true>(a, tile[b], nu, c0, r, rank, lane);
+        else
+            tile_pass<L, false>(a, tile[b], nu, c0, r, rank, lane);
+        __syncthreads();
+        if (tid == 0 && t + 2 < ntiles) {
+            const int32_t cn = c_lo + (t + 2) * kTileCols;
+            const int nun = (min(kTileCols, c_hi - cn) + U::kCols - 1) / U::kCols;
+            const uint32_t bytes = (uint32_t)nun * U::kBytes;
+            mbar_arrive_expect_tx(&bar[b], bytes);
+            bulk_g2s(&tile[b][0], units + (size_t)(cn / U::kCols) * U::kVec, bytes, &bar[b]);
+        }
+    }
+    if (r.ok)
+        a.counts[r.cell] = rank;
+}
+
+template <int... Ls>
+__device__ __forceinline__ void dispatch_item(int L, const PairArgs &a, const JobDesc &J, int band, int seg,
+                                              uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
+                                              bool &aborted, std::integer_sequence<int, Ls...>)
+{
+    ((L == Ls + 1 ? run_item<Ls + 1>(a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
+}
+
+__global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
+{
+    __shared__ __align__(128) uint4 tile[2][kSlotVec];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ long long item_sh;
 
     const int tid = threadIdx.x;
-    const int lane = tid & 31;
     if (tid == 0) {
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
@@ -258,107 +381,64 @@ __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
         const long long item = item_sh;
         if (item >= a.items || aborted)
             break;
-
-        // item -> (band, segment): bands are grouped by their first segment g;
-        // a band of group g owns segments g..nseg-1.
+        const JobDesc J = a.jobs[find_job_by_item(a.jobs, a.njobs, item)];
+        // local item -> (band, segment): bands are grouped by their first
+        // segment g; a band of group g owns segments g..nseg-1.
+        const long long li = item - J.item_off;
         int band = 0, seg = 0;
         {
             long long base = 0;
-            for (int g = 0; g < a.nseg; ++g) {
-                const int b_lo = g * a.bands_per_seg;
-                const int b_hi = min(b_lo + a.bands_per_seg, a.nbands);
-                const int per = a.nseg - g;
+            for (int g = 0; g < J.nseg; ++g) {
+                const int b_lo = g * J.bands_per_seg;
+                const int b_hi = min(b_lo + J.bands_per_seg, J.nbands);
+                const int per = J.nseg - g;
                 const long long cnt = (long long)max(b_hi - b_lo, 0) * per;
-                if (item < base + cnt) {
-                    const long long r = item - base;
-                    band = b_lo + (int)(r / per);
-                    seg = g + (int)(r % per);
+                if (li < base + cnt) {
+                    const long long q = li - base;
+                    band = b_lo + (int)(q / per);
+                    seg = g + (int)(q % per);
                     break;
                 }
                 base += cnt;
             }
         }
-        const int32_t row0 = band * kBandRows;
-        const int32_t row = row0 + tid;
-        const bool row_ok = row < a.n;
-        uint32_t p01, p23;
-        row_pools<L>(a.words[row_ok ? row : 0], p01, p23);
-        // c_lo is a multiple of 256 (segments and bands are), so units never
-        // straddle a segment
-        const int32_t c_lo = (int32_t)max((long long)seg << a.seg_shift, (long long)row0);
-        const int32_t c_hi = (int32_t)min((long long)(seg + 1) << a.seg_shift, (long long)a.n);
-        const long long row_end = (long long)row0 + kBandRows;
-        const bool check = ((long long)c_lo < row_end) || (row_end > (long long)a.n) ||
-                           (U::kCols == 2 && (c_hi & 1));
-        const int ntiles = (c_hi - c_lo + kTileCols - 1) / kTileCols;
-        uint32_t rank = 0;
-
-        if (tid == 0) {
-            for (int t = 0; t < 2 && t < ntiles; ++t) {
-                const int32_t c0 = c_lo + t * kTileCols;
-                const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
-                const uint32_t bytes = (uint32_t)nu * U::kBytes;
-                mbar_arrive_expect_tx(&bar[t], bytes);
-                bulk_g2s(&tile[t][0], a.units + (size_t)(c0 / U::kCols) * U::kVec, bytes, &bar[t]);
-            }
-        }
-        for (int t = 0; t < ntiles; ++t) {
-            const int b = t & 1;
-            bool timed_out = false;
-            const long long t_start = clock64();
-            while (!mbar_try_wait(&bar[b], (parity >> b) & 1u)) {
-                if (clock64() - t_start > kMaxWaitCycles) {
-                    timed_out = true;
-                    break;
-                }
-            }
-            parity ^= 1u << b;
-            // uniform decision: every thread leaves together if any gave up
-            if (__syncthreads_or(timed_out)) {
-                if (tid == 0)
-                    atomicExch(a.status, kStatusTimeout);
-                aborted = true;
-                break;
-            }
-            const int32_t c0 = c_lo + t * kTileCols;
-            const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
-            if (check)
-                tile_pass<L, true>(a, tile[b], nu, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
-            else
-                tile_pass<L, false>(a, tile[b], nu, c0, row, row_ok, p01, p23, (uint32_t)seg, rank, lane);
-            __syncthreads();
-            if (tid == 0 && t + 2 < ntiles) {
-                const int32_t cn = c_lo + (t + 2) * kTileCols;
-                const int nun = (min(kTileCols, c_hi - cn) + U::kCols - 1) / U::kCols;
-                const uint32_t bytes = (uint32_t)nun * U::kBytes;
-                mbar_arrive_expect_tx(&bar[b], bytes);
-                bulk_g2s(&tile[b][0], a.units + (size_t)(cn / U::kCols) * U::kVec, bytes, &bar[b]);
-            }
-        }
+        dispatch_item(J.L, a, J, band, seg, tile, bar, parity, aborted,
+                      std::make_integer_sequence<int, IG_MAX_LEN>{});
         if (aborted)
             break;
-        if (row_ok)
-            a.counts[(size_t)seg * (size_t)a.n + (size_t)row] = rank;
         __syncthreads();
     }
 }
 
 // Per row: in-place exclusive prefix of its segment counts; degree -> out[row+1].
-__global__ void row_prefix(uint32_t *__restrict__ counts, int32_t n, int nseg, int seg_shift,
-                           int64_t *__restrict__ out)
+__global__ void row_prefix(uint32_t *__restrict__ counts, const JobDesc *__restrict__ jobs, int njobs,
+                           int64_t rows, int64_t *__restrict__ out)
 {
-    const int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (row >= n)
+    const int64_t gr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (gr >= rows)
         return;
-    const int g = (int)(((row / kBandRows) * kBandRows) >> seg_shift);
+    const JobDesc J = jobs[find_job_by_row(jobs, njobs, gr)];
+    const int64_t row = gr - J.word_off;
+    const int g = (int)(((row / kBandRows) * kBandRows) >> J.seg_shift);
     uint32_t acc = 0;
-    for (int s = g; s < nseg; ++s) {
-        uint32_t *p = counts + (size_t)s * (size_t)n + (size_t)row;
+    for (int s = g; s < J.nseg; ++s) {
+        uint32_t *p = counts + J.count_off + (int64_t)s * J.n + row;
         const uint32_t c = *p;
         *p = acc;
         acc += c;
     }
-    out[row + 1] = (int64_t)acc;
+    out[gr + 1] = (int64_t)acc;
+}
+
+// Row offsets at job boundaries: out[j] = row_ptr[word_off_j], out[k] = row_ptr[rows].
+__global__ void job_bounds(const int64_t *__restrict__ row_ptr, const JobDesc *__restrict__ jobs, int njobs,
+                           int64_t rows, int64_t *__restrict__ out)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < njobs)
+        out[j] = row_ptr[jobs[j].word_off];
+    else if (j == njobs)
+        out[j] = row_ptr[rows];
 }
 
 // ---- inclusive scan of int64 in place: block scan, scan of block sums, add ----
@@ -449,49 +529,15 @@ __global__ void scan_add(int64_t *__restrict__ x, int64_t m, const int64_t *__re
 }
 
 __global__ void scatter_records(const EdgeRecord *__restrict__ rec, unsigned long long nrec,
-                                const int64_t *__restrict__ row_ptr, const uint32_t *__restrict__ counts, int32_t n,
+                                const int64_t *__restrict__ row_ptr, const uint32_t *__restrict__ counts,
                                 int32_t *__restrict__ cols)
 {
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < nrec;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const uint4 r = *reinterpret_cast<const uint4 *>(rec + i);
-        const int64_t pos = row_ptr[r.x] + (int64_t)counts[(size_t)r.w * (size_t)n + r.x] + (int64_t)r.z;
+        const int64_t pos = row_ptr[r.x] + (int64_t)counts[r.w] + (int64_t)r.z;
         cols[pos] = (int32_t)r.y;
     }
-}
-
-template <int L>
-void launch_pairs(const PairArgs &a, int grid, cudaStream_t st)
-{
-    pair_kernel<L><<<grid, kBandRows, 0, st>>>(a);
-}
-
-typedef void (*pairs_launcher)(const PairArgs &, int, cudaStream_t);
-typedef const void *kernel_ptr;
-
-template <int L>
-const void *pairs_kernel_ptr()
-{
-    return reinterpret_cast<const void *>(&pair_kernel<L>);
-}
-
-struct PairTable {
-    pairs_launcher launch[IG_MAX_LEN + 1];
-    kernel_ptr kern[IG_MAX_LEN + 1];
-};
-
-template <int... Ls>
-PairTable make_table(std::integer_sequence<int, Ls...>)
-{
-    PairTable t{};
-    ((t.launch[Ls + 1] = &launch_pairs<Ls + 1>, t.kern[Ls + 1] = pairs_kernel_ptr<Ls + 1>()), ...);
-    return t;
-}
-
-const PairTable &pair_table()
-{
-    static const PairTable t = make_table(std::make_integer_sequence<int, IG_MAX_LEN>{});
-    return t;
 }
 
 ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
@@ -522,39 +568,84 @@ ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
             return cuda_error(ctx, e_, #call);                                                                 \
     } while (0)
 
-int pair_grid(Ctx *ctx, int len)
+int pair_grid(Ctx *ctx)
 {
-    int bps = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pair_table().kern[len], kBandRows, 0);
-    if (bps < 1)
-        bps = 1;
-    return bps * ctx->sm_count;
+    if (ctx->pair_grid == 0) {
+        int bps = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pair_kernel, kBandRows, 0);
+        cudaGetLastError();
+        ctx->pair_grid = std::max(bps, 1) * ctx->sm_count;
+    }
+    return ctx->pair_grid;
 }
 
-// Runs prep + the pair kernel.  On return *total holds the number of edges;
-// records are complete iff *total <= capacity.
-ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, const PairPlan &plan,
-                    int grid, int emit, unsigned long long *total)
+// Device-side layout of a batch.
+struct BatchLayout {
+    std::vector<JobDesc> desc;
+    long long items = 0;
+    long long units = 0;       // column units over all jobs
+    long long unit_vec = 0;    // uint4 of all unit streams
+    long long counts = 0;      // per-(segment, row) cells
+    int64_t rows = 0;
+};
+
+bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
+{
+    long double pairs_total = 0;
+    for (const JobSpec &j : jobs)
+        pairs_total += (long double)j.n * (j.n > 0 ? j.n - 1 : 0) / 2;
+    const long long want_items = 24ll * grid;
+    out = BatchLayout();
+    for (const JobSpec &j : jobs) {
+        JobDesc d{};
+        const long double share = pairs_total > 0 ? ((long double)j.n * (j.n - 1) / 2) / pairs_total : 0;
+        const PairPlan p = make_plan(j.n, std::max<long long>(1, (long long)(share * want_items)));
+        d.word_off = j.word_off;
+        d.n = j.n;
+        d.L = j.len;
+        d.lim = std::max(-64, std::min(64, j.min_ed - j.len));
+        d.seg_shift = p.seg_shift;
+        d.nseg = p.nseg;
+        d.bands_per_seg = p.bands_per_seg;
+        d.nbands = p.nbands;
+        d.item_off = out.items;
+        d.unit_start = out.units;
+        d.unit_off = out.unit_vec;
+        d.count_off = out.counts;
+        const long long units = j.len <= 15 ? ((long long)j.n + 1) / 2 : (long long)j.n;
+        out.items += j.n >= 2 ? p.items : 0;
+        out.units += units;
+        out.unit_vec += units * (j.len <= 15 ? 4 : 2);
+        out.counts += (long long)p.nseg * j.n;
+        out.rows = std::max<int64_t>(out.rows, j.word_off + j.n);
+        out.desc.push_back(d);
+    }
+    return out.counts < (1ll << 32);
+}
+
+// Runs prep + the pair kernel for a planned batch.  On return *total holds
+// the number of edges; records are complete iff *total <= capacity.
+ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int grid, int emit,
+                    unsigned long long *total)
 {
     cudaStream_t st = ctx->stream;
     ig_status s;
-    const bool two = len <= 15;
-    const size_t unit_bytes = two ? 64 : 32;
-    const size_t units = two ? ((size_t)n + 1) / 2 : (size_t)n;
-    if ((s = ensure(ctx, ctx->sel, units * unit_bytes, "column streams")) != IG_OK)
+    if ((s = ensure(ctx, ctx->sel, (size_t)B.unit_vec * sizeof(uint4), "column streams")) != IG_OK)
         return s;
-    if ((s = ensure(ctx, ctx->counts, (size_t)plan.nseg * (size_t)n * sizeof(uint32_t), "segment counts")) !=
-        IG_OK)
+    if ((s = ensure(ctx, ctx->counts, (size_t)B.counts * sizeof(uint32_t), "segment counts")) != IG_OK)
         return s;
     if ((s = ensure(ctx, ctx->flags, 4 * sizeof(unsigned long long), "flags")) != IG_OK)
         return s;
+    const size_t jbytes = B.desc.size() * sizeof(JobDesc);
+    if ((s = ensure(ctx, ctx->jobs, jbytes + (B.desc.size() + 1) * sizeof(int64_t), "job table")) != IG_OK)
+        return s;
+    IG_CUDA(cudaMemcpyAsync(ctx->jobs.ptr, B.desc.data(), jbytes, cudaMemcpyHostToDevice, st));
+    const JobDesc *d_jobs = static_cast<const JobDesc *>(ctx->jobs.ptr);
+    const int njobs = (int)B.desc.size();
     phase_begin(ctx, IG_PHASE_PREP);
-    if (two)
-        prep_units2<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(d_words, n, len,
-                                                                     static_cast<uint4 *>(ctx->sel.ptr));
-    else
-        prep_units1<<<(unsigned)((units + 255) / 256), 256, 0, st>>>(d_words, n, len,
-                                                                     static_cast<uint4 *>(ctx->sel.ptr));
+    if (B.units > 0)
+        prep_units<<<(unsigned)((B.units + 255) / 256), 256, 0, st>>>(d_words, d_jobs, njobs, B.units,
+                                                                       static_cast<uint4 *>(ctx->sel.ptr));
     phase_end(ctx, IG_PHASE_PREP);
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
@@ -563,17 +654,12 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
     PairArgs a;
     a.units = static_cast<const uint4 *>(ctx->sel.ptr);
     a.words = d_words;
-    a.n = n;
-    // min_ed <= 0: no pair can be an edge; min_ed > L: every pair is one
-    a.lim = (int)std::max(-64, std::min(64, min_ed - len));
+    a.jobs = d_jobs;
+    a.njobs = njobs;
+    a.items = B.items;
     a.one = 1u;
     a.two = 2u;
     a.hi = 1u << 16;
-    a.seg_shift = plan.seg_shift;
-    a.nseg = plan.nseg;
-    a.bands_per_seg = plan.bands_per_seg;
-    a.nbands = plan.nbands;
-    a.items = plan.items;
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);
@@ -582,7 +668,7 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
     a.emit = emit;
     phase_begin(ctx, IG_PHASE_PAIRS);
-    pair_table().launch[len](a, grid, st);
+    pair_kernel<<<grid, kBandRows, 0, st>>>(a);
     phase_end(ctx, IG_PHASE_PAIRS);
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
@@ -593,6 +679,19 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int m
     if (static_cast<int>(host_flags[2] & 0xffffffffu) == kStatusTimeout)
         return set_error(ctx, IG_ERR_TIMEOUT, "pair kernel: staged tile never arrived (bounded wait expired)");
     *total = host_flags[1];
+    return IG_OK;
+}
+
+ig_status check_jobs(Ctx *ctx, const std::vector<JobSpec> &jobs)
+{
+    int64_t rows = 0;
+    for (const JobSpec &j : jobs) {
+        if (j.n < 0 || j.len < 1 || j.len > IG_MAX_LEN || j.word_off < 0)
+            return set_error(ctx, IG_ERR_INPUT, "job: n >= 0 and 1 <= len <= 16 required");
+        rows = std::max<int64_t>(rows, j.word_off + j.n);
+    }
+    if (rows > (int64_t)INT32_MAX)
+        return set_error(ctx, IG_ERR_CAPACITY, "more than 2^31-1 words in one batch");
     return IG_OK;
 }
 
@@ -648,26 +747,25 @@ void phase_collect(Ctx *ctx)
     }
 }
 
-PairPlan make_plan(int32_t n, int grid_ctas)
+PairPlan make_plan(int32_t n, long long target_items)
 {
     PairPlan p;
     p.n = n;
-    // Segment width: a power of two >= one band, small enough that the queue
-    // holds many items per CTA, large enough that at most 256 segments exist
-    // and the per-(row, segment) counts stay under 1 GiB.
+    // Segment width: a power of two >= one band, small enough that the job
+    // yields about target_items items, large enough that at most 256 segments
+    // exist and the per-(row, segment) counts stay under 1 GiB.
     int shift = 8;  // 256 columns
     while (((int64_t)n + (1ll << shift) - 1) >> shift > 256)
         shift++;
     while ((((int64_t)n + (1ll << shift) - 1) >> shift) * (int64_t)n * 4 > (1ll << 30))
         shift++;
-    // Prefer wider segments (fewer per-item overheads) while the queue keeps
-    // at least 24 items per CTA.
+    // Prefer wider segments (fewer per-item overheads) while the target holds.
     for (;;) {
         const int s2 = shift + 1;
         const int64_t nseg2 = ((int64_t)n + (1ll << s2) - 1) >> s2;
         const int64_t nb = ((int64_t)n + kBandRows - 1) / kBandRows;
         const int64_t items2 = nb * (nseg2 + 1) / 2;
-        if (s2 > 14 || items2 < 24ll * grid_ctas)
+        if (s2 > 14 || items2 < target_items)
             break;
         shift = s2;
     }
@@ -685,47 +783,58 @@ PairPlan make_plan(int32_t n, int grid_ctas)
     return p;
 }
 
-ig_status count_edges(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, int64_t *edges)
+ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int64_t *edges)
 {
-    if (n < 2) {
+    ig_status s = check_jobs(ctx, jobs);
+    if (s != IG_OK)
+        return s;
+    const int grid = pair_grid(ctx);
+    BatchLayout B;
+    if (!plan_batch(jobs, grid, B))
+        return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
+    if (B.items == 0) {
         *edges = 0;
         return IG_OK;
     }
-    const int grid = pair_grid(ctx, len);
-    const PairPlan plan = make_plan(n, grid);
     unsigned long long total = 0;
-    ig_status s = run_pairs(ctx, d_words, n, len, min_ed, plan, grid, 0, &total);
+    s = run_pairs(ctx, d_words, B, grid, 0, &total);
     if (s != IG_OK)
         return s;
     *edges = (int64_t)total;
     return IG_OK;
 }
 
-ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, Graph *g)
+ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, Graph *g)
 {
     cudaStream_t st = ctx->stream;
+    ig_status s = check_jobs(ctx, jobs);
+    if (s != IG_OK)
+        return s;
+    const int grid = pair_grid(ctx);
+    BatchLayout B;
+    if (!plan_batch(jobs, grid, B))
+        return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
+    const int32_t n = (int32_t)B.rows;
     g->ctx = ctx;
     g->n = n;
-    g->len = len;
-    g->min_ed = min_ed;
+    g->jobs = jobs;
+    g->job_edge_off.assign(jobs.size() + 1, 0);
     IG_CUDA(cudaMallocAsync((void **)&g->d_row_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
-    if (n < 2) {
+    if (B.items == 0) {
         IG_CUDA(cudaMemsetAsync(g->d_row_ptr, 0, ((size_t)n + 1) * sizeof(int64_t), st));
         IG_CUDA(cudaStreamSynchronize(st));
         g->edges = 0;
         return IG_OK;
     }
-    const int grid = pair_grid(ctx, len);
-    const PairPlan plan = make_plan(n, grid);
     if (ctx->rec_capacity == 0) {
-        ig_status s = ensure(ctx, ctx->records, (size_t)(1u << 22) * sizeof(EdgeRecord), "edge records");
+        s = ensure(ctx, ctx->records, (size_t)(1u << 22) * sizeof(EdgeRecord), "edge records");
         if (s != IG_OK)
             return s;
         ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
     }
     unsigned long long total = 0;
     for (int attempt = 0;; ++attempt) {
-        ig_status s = run_pairs(ctx, d_words, n, len, min_ed, plan, grid, 1, &total);
+        s = run_pairs(ctx, d_words, B, grid, 1, &total);
         if (s != IG_OK)
             return s;
         if (total <= ctx->rec_capacity)
@@ -741,29 +850,36 @@ ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int
     g->edges = (int64_t)total;
     IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
     IG_CUDA(cudaMemsetAsync(g->d_row_ptr, 0, sizeof(int64_t), st));
+    const JobDesc *d_jobs = static_cast<const JobDesc *>(ctx->jobs.ptr);
+    const int njobs = (int)B.desc.size();
     phase_begin(ctx, IG_PHASE_COMPACT);
-    row_prefix<<<(n + 255) / 256, 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr), n, plan.nseg,
-                                                  plan.seg_shift, g->d_row_ptr);
+    row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr), d_jobs, njobs,
+                                                               n, g->d_row_ptr);
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
     // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
-    ig_status s = inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1);
+    s = inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1);
     if (s != IG_OK)
         return s;
     if (total > 0) {
-        const int sgrid = (int)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)ctx->sm_count * 16);
+        const int sgrid =
+            (int)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)ctx->sm_count * 16);
         scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), total,
-                                                g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr), n,
+                                                g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
                                                 g->d_cols);
         ctx->launches++;
         IG_CUDA(cudaGetLastError());
     }
     phase_end(ctx, IG_PHASE_COMPACT);
-    int64_t last = -1;
-    IG_CUDA(cudaMemcpyAsync(&last, g->d_row_ptr + n, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    int64_t *d_bounds = reinterpret_cast<int64_t *>(static_cast<char *>(ctx->jobs.ptr) + B.desc.size() * sizeof(JobDesc));
+    job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, d_jobs, njobs, n, d_bounds);
+    ctx->launches++;
+    IG_CUDA(cudaGetLastError());
+    IG_CUDA(cudaMemcpyAsync(g->job_edge_off.data(), d_bounds, (njobs + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                            st));
     IG_CUDA(cudaStreamSynchronize(st));
     phase_collect(ctx);
-    if (last != (int64_t)total)
+    if (g->job_edge_off[(size_t)njobs] != (int64_t)total)
         return set_error(ctx, IG_ERR_STATE, "row offsets disagree with the edge count");
     return IG_OK;
 }

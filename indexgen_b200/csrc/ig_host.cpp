@@ -23,10 +23,21 @@ namespace {
 // followed -- when t = x mod T -- by all upper neighbours ascending.  T = 1 is
 // the fully sorted order AdjList::FromBinaryFile builds from a row-sorted
 // edge file (src/SparseMat.cpp:338-390).
-void assemble(const int64_t *row_ptr, const int32_t *cols, int32_t n, int T, std::vector<int64_t> &ap,
-              std::vector<int32_t> &adj)
+// row_ptr covers the job's n rows (its values index cols); column ids are
+// global and `base` maps them to job-local ids.  The output is job-local.
+void assemble(const int64_t *row_ptr, const int32_t *cols_in, int32_t n, int64_t base, int T,
+              std::vector<int64_t> &ap, std::vector<int32_t> &adj)
 {
-    const int64_t nnz = row_ptr[n];
+    const int64_t first = row_ptr[0];
+    const int64_t nnz = row_ptr[n] - first;
+    std::vector<int32_t> local((size_t)std::max<int64_t>(nnz, 1));
+    for (int64_t k = 0; k < nnz; ++k)
+        local[(size_t)k] = (int32_t)(cols_in[first + k] - base);
+    std::vector<int64_t> rp((size_t)n + 1);
+    for (int32_t i = 0; i <= n; ++i)
+        rp[(size_t)i] = row_ptr[i] - first;
+    const int32_t *cols = local.data();
+    row_ptr = rp.data();
     std::vector<int64_t> lp((size_t)n + 1, 0);
     for (int64_t k = 0; k < nnz; ++k)
         lp[(size_t)cols[k] + 1]++;
@@ -92,7 +103,10 @@ void assemble(const int64_t *row_ptr, const int32_t *cols, int32_t n, int T, std
 // actually used are ever touched.
 class BucketGreedy {
   public:
-    BucketGreedy(const int64_t *ap, const int32_t *adj, int32_t n) : ap_(ap), adj_(adj), v_((size_t)n)
+    // ap covers the n job rows (its values index adj); neighbour ids in adj
+    // are global and `base` maps them to job-local ids.
+    BucketGreedy(const int64_t *ap, const int32_t *adj, int32_t n, int64_t base)
+        : ap_(ap), adj_(adj), base_(base), v_((size_t)n)
     {
         int32_t maxd = 0;
         for (int32_t i = 0; i < n; ++i) {
@@ -137,7 +151,7 @@ class BucketGreedy {
             todel_.resize((size_t)(e - b) + 1);
             int32_t nt = 0;
             for (int64_t k = b; k < e; ++k) {  // branch-free compaction
-                const int32_t j = adj_[k];
+                const int32_t j = (int32_t)(adj_[k] - base_);
                 todel_[(size_t)nt] = j;
                 nt += v_[(size_t)j].deg >= 0;
             }
@@ -189,7 +203,7 @@ class BucketGreedy {
             int32_t jj[8], dd[8];
             unsigned live = 0;
             for (int t = 0; t < m; ++t) {
-                jj[t] = adj_[k + t];
+                jj[t] = (int32_t)(adj_[k + t] - base_);
                 dd[t] = v_[(size_t)jj[t]].deg;
             }
             for (int t = 0; t < m; ++t)
@@ -211,6 +225,7 @@ class BucketGreedy {
     };
     const int64_t *ap_;
     const int32_t *adj_;
+    int64_t base_;
     std::vector<Vtx> v_;
     std::vector<int32_t> size_;
     std::vector<int64_t> start_;
@@ -223,23 +238,23 @@ class BucketGreedy {
 
 }  // namespace
 
-int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
+int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int64_t base, int order_threads,
                           int32_t *order)
 {
     if (n <= 0)
         return 0;
     std::vector<int64_t> ap;
     std::vector<int32_t> adj;
-    assemble(row_ptr, cols, n, order_threads, ap, adj);
-    BucketGreedy g(ap.data(), adj.data(), n);
+    assemble(row_ptr, cols, n, base, order_threads, ap, adj);
+    BucketGreedy g(ap.data(), adj.data(), n, 0);
     return g.run(order);
 }
 
-int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order)
+int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int64_t base, int32_t *order)
 {
     if (n <= 0)
         return 0;
-    BucketGreedy g(adj_ptr, adj, n);
+    BucketGreedy g(adj_ptr, adj, n, base);
     return g.run(order);
 }
 
@@ -321,7 +336,7 @@ ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols
         if (cols[k] < 0 || cols[k] >= n)
             return IG_ERR_INPUT;
     try {
-        *count = ig::greedy_from_upper(row_ptr, cols, n, order_threads, order);
+        *count = ig::greedy_from_upper(row_ptr, cols, n, 0, order_threads, order);
     } catch (...) {
         return IG_ERR_OOM;
     }

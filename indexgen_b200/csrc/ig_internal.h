@@ -16,10 +16,32 @@ namespace ig {
 constexpr int kBandRows = 256;
 constexpr int kTileCols = 256;
 
-// One emitted edge: (row, col, rank of col inside (row, segment), segment).
+// One emitted edge: global row, global column, rank of the column among the
+// row's hits in its (row, segment) cell, and the index of that cell's count.
 // Ranks make the CSR scatter order-exact without a sort.
 struct EdgeRecord {
-    uint32_t row, col, rank, seg;
+    uint32_t row, col, rank, cell;
+};
+
+// One job of a batch as the device sees it.  Rows and columns of a job are
+// local (0..n-1); word_off maps them to the concatenated word array.
+struct JobDesc {
+    int64_t word_off;    // first word of the job (global row/column base)
+    int64_t unit_off;    // first uint4 of the job's column-unit stream
+    int64_t unit_start;  // first unit (prefix over jobs, in units)
+    int64_t item_off;    // first (band, segment) work item (prefix over jobs)
+    int64_t count_off;   // first per-(segment, row) count ([nseg][n] block)
+    int32_t n, L, lim;   // words, length, min_ed - L
+    int32_t seg_shift, nseg, bands_per_seg, nbands;
+    int32_t pad;
+};
+
+// Host description of a job.
+struct JobSpec {
+    int64_t word_off = 0;
+    int32_t n = 0;
+    int32_t len = 1;
+    int32_t min_ed = 0;
 };
 
 // Grow-only device buffer owned by a context.
@@ -36,8 +58,9 @@ struct Ctx {
     std::string last_error;
     int64_t launches = 0;
     // workspace
-    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp;
+    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs;
     unsigned long long rec_capacity = 0;  // records that fit in `records`
+    int pair_grid = 0;                    // persistent CTAs of the pair kernel
     // optional per-phase timing (IG_PHASE_*)
     bool profiling = false;
     cudaEvent_t ev[6] = {};
@@ -53,12 +76,12 @@ void phase_collect(Ctx *ctx);  // after a stream sync: fold finished pairs in
 
 struct Graph {
     Ctx *ctx = nullptr;
-    int32_t n = 0;
-    int len = 0;
-    int min_ed = 0;
+    int32_t n = 0;                      // rows over all jobs
     int64_t edges = 0;
-    int64_t *d_row_ptr = nullptr;  // [n+1]
-    int32_t *d_cols = nullptr;     // [edges]
+    std::vector<JobSpec> jobs;          // one entry for a single-job graph
+    std::vector<int64_t> job_edge_off;  // [jobs+1] row_ptr at job boundaries
+    int64_t *d_row_ptr = nullptr;       // [n+1]
+    int32_t *d_cols = nullptr;          // [edges], global column ids
     // host copies, filled on first use
     std::vector<int64_t> h_row_ptr;
     std::vector<int32_t> h_cols;
@@ -78,11 +101,12 @@ struct PairPlan {
     long long items = 0;   // (band, segment) work items in the upper triangle
 };
 
-PairPlan make_plan(int32_t n, int grid_ctas);
+// Plan for a job of n words that should yield about `target_items` items.
+PairPlan make_plan(int32_t n, long long target_items);
 
-// Device pipeline stages (ig_graph.cu).
-ig_status build_graph(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, Graph *g);
-ig_status count_edges(Ctx *ctx, const uint32_t *d_words, int32_t n, int len, int min_ed, int64_t *edges);
+// Device pipeline stages (ig_graph.cu).  Jobs index into d_words.
+ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, Graph *g);
+ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int64_t *edges);
 
 // In-place inclusive scan of m int64 on the context stream (ig_graph.cu).
 ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m);
@@ -90,11 +114,13 @@ ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what);
 // Symmetric CSR in the canonical neighbour order (ig_adjacency.cu).
 ig_status build_adjacency(Ctx *ctx, Graph *g);
 
-// Host greedy (ig_host.cpp).
-int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
+// Host greedy (ig_host.cpp).  Vertex ids in cols / adj are global; `base`
+// is subtracted to get the job-local ids the greedy works with and returns.
+int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int64_t base, int order_threads,
                           int32_t *order);
 // Greedy directly over neighbour lists already in m-order.
-int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order);
+int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int64_t base,
+                              int32_t *order);
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);

@@ -143,6 +143,34 @@ class ConflictGraph:
               "ig_graph_codebook", self.ctx.handle)
         return order[: cnt.value]
 
+    @property
+    def jobs(self) -> int:
+        k = ctypes.c_int32()
+        check(lib().ig_graph_job_count(self.handle, ctypes.byref(k)), "ig_graph_job_count")
+        return int(k.value)
+
+    def job_stats(self, job: int):
+        """(first word, n, edges) of one job of a batch graph."""
+        f = ctypes.c_int64()
+        n = ctypes.c_int32()
+        e = ctypes.c_int64()
+        check(lib().ig_graph_job_stats(self.handle, int(job), ctypes.byref(f), ctypes.byref(n), ctypes.byref(e)),
+              "ig_graph_job_stats")
+        return int(f.value), int(n.value), int(e.value)
+
+    def job_codebooks(self, order_threads: int = 1, host_threads: int = 0):
+        """Per-job codebooks (job-local ids in selection order), as a list."""
+        k = self.jobs
+        order = np.zeros(max(self.n, 1), np.int32)
+        counts = np.zeros(max(k, 1), np.int32)
+        check(lib().ig_graph_job_codebooks(self.handle, int(order_threads), int(host_threads), ptr(order),
+                                           ptr(counts)), "ig_graph_job_codebooks", self.ctx.handle)
+        out = []
+        for j in range(k):
+            f, _, _ = self.job_stats(j)
+            out.append(order[f:f + counts[j]].copy())
+        return out
+
     def adj_list(self):
         """Neighbour lists in both directions, ascending (list of lists)."""
         adj_ptr, adj = self.adjacency()
@@ -181,6 +209,45 @@ def build_conflict_graph(words, L: int, min_ed: int, ctx: Context | None = None)
         check(lib().ig_graph_build(ctx.handle, ptr(w), len(w), int(L), int(min_ed), 0, ctypes.byref(h)),
               "ig_graph_build", ctx.handle)
     return ConflictGraph(h, ctx, int(L), int(min_ed))
+
+
+def _batch_arrays(jobs):
+    """jobs: iterable of (words, L, min_ed) -> concatenated words, offsets, lens, min_eds."""
+    ws, lens, eds = [], [], []
+    for w, L, d in jobs:
+        ws.append(_words_array(w))
+        lens.append(int(L))
+        eds.append(int(d))
+    offsets = np.zeros(len(ws) + 1, np.int64)
+    if ws:
+        offsets[1:] = np.cumsum([len(w) for w in ws])
+    words = np.concatenate(ws) if ws else np.zeros(0, np.uint32)
+    return np.ascontiguousarray(words), offsets, np.asarray(lens, np.int32), np.asarray(eds, np.int32)
+
+
+def build_batch(jobs, ctx: Context | None = None) -> ConflictGraph:
+    """One block-diagonal conflict graph for a list of (words, L, min_ed) jobs,
+    built by one device pipeline (one persistent pair-test launch)."""
+    ctx = ctx or default_context()
+    words, offsets, lens, eds = _batch_arrays(jobs)
+    h = ctypes.c_void_p()
+    check(lib().ig_batch_build(ctx.handle, ptr(words), ptr(offsets), len(lens), ptr(lens), ptr(eds), 0,
+                               ctypes.byref(h)), "ig_batch_build", ctx.handle)
+    return ConflictGraph(h, ctx, 0, 0)
+
+
+def solve_batch(jobs, order_threads: int = 1, host_threads: int = 0, ctx: Context | None = None):
+    """Codebooks (job-local ids in selection order) and edge counts of a batch."""
+    ctx = ctx or default_context()
+    words, offsets, lens, eds = _batch_arrays(jobs)
+    k = len(lens)
+    order = np.zeros(max(len(words), 1), np.int32)
+    counts = np.zeros(max(k, 1), np.int32)
+    edges = np.zeros(max(k, 1), np.int64)
+    check(lib().ig_solve_batch(ctx.handle, ptr(words), ptr(offsets), k, ptr(lens), ptr(eds), int(order_threads),
+                               int(host_threads), ptr(order), ptr(counts), ptr(edges)), "ig_solve_batch",
+          ctx.handle)
+    return [order[offsets[j]:offsets[j] + counts[j]].copy() for j in range(k)], edges[:k].copy()
 
 
 def count_conflicts(words, L: int, min_ed: int, ctx: Context | None = None) -> int:
@@ -293,7 +360,8 @@ def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
 
 
 __all__ = [
-    "Context", "ConflictGraph", "IndexGenError", "build_conflict_graph", "count_conflicts",
+    "Context", "ConflictGraph", "IndexGenError", "build_conflict_graph", "build_batch", "solve_batch",
+    "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context",
 ]

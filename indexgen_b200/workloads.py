@@ -186,3 +186,72 @@ def linear12_candidates() -> np.ndarray:
 def uniform11_candidates() -> np.ndarray:
     """The CPU-runnable workload: 20,000 uniform n=11 strings (seed 12345), filtered."""
     return uniform_filtered(20000, 11, 12345, max_run=3, min_gc=0.3, max_gc=0.7)
+
+
+def zipf_sizes(total: int, k: int, s: float = 1.1, lo: int = 2000, hi: int = 60000) -> np.ndarray:
+    """k cluster sizes proportional to i^-s (i = 1..k), clamped to [lo, hi] and
+    renormalised so they sum to `total` (clamped sizes stay at their bound,
+    the free ones absorb the rest; integer rounding by largest remainder)."""
+    if not lo * k <= total <= hi * k:
+        raise ValueError("total must lie in [lo*k, hi*k]")
+    w = np.arange(1, k + 1, dtype=np.float64) ** -s
+    size = w / w.sum() * total
+    fixed = np.zeros(k, bool)
+    for _ in range(4 * k):
+        free = ~fixed
+        rest = total - size[fixed].sum()
+        size[free] = w[free] / w[free].sum() * rest
+        over = free & ((size > hi) | (size < lo))
+        if not over.any():
+            break
+        size[over] = np.clip(size[over], lo, hi)
+        fixed |= over
+    base = np.floor(size).astype(np.int64)
+    short = int(total - base.sum())
+    order = np.argsort(-(size - base), kind="stable")
+    base[order[:short]] += 1
+    return base
+
+
+def assign_clusters(words, L: int, sizes, seed: int):
+    """Capacity-constrained nearest-centre assignment (a k-means-style step
+    with imposed sizes).  Centres are seeded random members; clusters, largest
+    first, take their `size` nearest unassigned words by Hamming distance to
+    the centre (ties by word index).  Returns one index array per cluster, in
+    ascending word order."""
+    w = np.asarray(words, np.uint32)
+    n = len(w)
+    sizes = np.asarray(sizes, np.int64)
+    if sizes.sum() != n:
+        raise ValueError("sizes must sum to the number of words")
+    rng = np.random.default_rng(seed)
+    centres = w[rng.choice(n, len(sizes), replace=False)]
+    digits = unpack_digits(w, L)
+    free = np.ones(n, bool)
+    out = [None] * len(sizes)
+    for c in np.argsort(-sizes, kind="stable"):
+        cd = unpack_digits(centres[c:c + 1], L)[0]
+        dist = (digits != cd[None, :]).sum(axis=1)
+        need = int(sizes[c])
+        take = []
+        for d in range(L + 1):
+            idx = np.nonzero(free & (dist == d))[0]
+            if len(idx) >= need:
+                take.append(idx[:need])
+                need = 0
+                break
+            take.append(idx)
+            need -= len(idx)
+        sel = np.sort(np.concatenate(take))
+        free[sel] = False
+        out[c] = sel
+    return out
+
+
+def clustered14(total: int = 1_000_000, k: int = 64, seed: int = 14):
+    """The batched-clusters workload: `total` filtered uniform n=14 words split
+    into k clusters with Zipf(1.1) sizes in [2000, 60000].  Returns a list of
+    packed word arrays, one per cluster."""
+    w = uniform_until(total, 14, seed, max_run=3, min_gc=0.3, max_gc=0.7)
+    parts = assign_clusters(w, 14, zipf_sizes(total, k), seed + 1)
+    return [w[p] for p in parts]

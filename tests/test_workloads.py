@@ -60,3 +60,18 @@ def test_vt16_membership():
     assert np.all((d * np.arange(1, 17)).sum(axis=1) % 17 == 0)
     assert np.all(d.sum(axis=1) % 4 == 0)
     assert W.filter_words(w, 16).all()
+
+
+def test_zipf_sizes():
+    s = W.zipf_sizes(1_000_000, 64)
+    assert s.sum() == 1_000_000 and s.min() >= 2000 and s.max() <= 60000
+    assert np.all(np.diff(s) <= 0)
+
+
+def test_assign_clusters_partition():
+    w = W.uniform_until(5000, 14, 9)
+    parts = W.assign_clusters(w, 14, W.zipf_sizes(5000, 8, lo=100, hi=2000), 10)
+    allidx = np.concatenate(parts)
+    assert len(allidx) == 5000 and len(np.unique(allidx)) == 5000
+    again = W.assign_clusters(w, 14, W.zipf_sizes(5000, 8, lo=100, hi=2000), 10)
+    assert all(np.array_equal(a, b) for a, b in zip(parts, again))
