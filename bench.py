@@ -263,6 +263,66 @@ def run_batch_section(ctx, reps: int = 3) -> dict:
             "note": "wall clock through solve_batch vs a loop of solve (graph + greedy per cluster)"}
 
 
+def run_serve_section(ctx, jobs: int, nmax: int, rate: float = 50.0) -> dict:
+    """Serving stream: seeded Poisson arrivals (mean `rate` jobs/s), n uniform
+    in 10..16, editDist uniform in 3..5, candidates log-uniform in [5k, nmax].
+    The continuous-batching server (all host cores for greedies) against the
+    plain one-job-per-launch path (one worker solving jobs in arrival order).
+    Latency = arrival to codebook ready."""
+    import threading
+
+    from indexgen_b200 import Server, solve
+
+    stream = W.serving_stream(jobs, seed=5, rate=rate, nmin=5000, nmax=nmax)
+    pairs = sum(len(w) * (len(w) - 1) // 2 for _, w, _, _ in stream)
+    solve(stream[0][1], stream[0][2], stream[0][3], 1, ctx)  # warm-up
+    cores = host_cores()
+
+    # served
+    lat = [0.0] * len(stream)
+    results = [None] * len(stream)
+    with Server(ctx, host_threads=cores) as sv:
+        tickets = [None] * len(stream)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i, (arr, w, L, d) in enumerate(stream):
+                dt = arr - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = sv.submit(w, L, d)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for i in range(len(stream)):
+            order, _, ms = sv.wait(tickets[i])
+            lat[i] = ms
+            results[i] = order
+        t_served = time.perf_counter() - t0
+        st = sv.stats()
+    # plain: one job per launch, in arrival order
+    lat_plain = []
+    same = True
+    t0 = time.perf_counter()
+    for i, (arr, w, L, d) in enumerate(stream):
+        dt = arr - (time.perf_counter() - t0)
+        if dt > 0:
+            time.sleep(dt)
+        order, _ = solve(w, L, d, 1, ctx)
+        lat_plain.append(1e3 * (time.perf_counter() - t0 - arr))
+        same = same and np.array_equal(order, results[i])
+    t_plain = time.perf_counter() - t0
+    return {"workload": f"{jobs} jobs, Poisson {rate:g}/s, n 10..16, editDist 3..5, candidates log-uniform "
+                        f"[5000, {nmax}] (seed 5)",
+            "pair_tests": pairs, "served_jobs_per_s": len(stream) / t_served,
+            "served_p50_ms": float(np.percentile(lat, 50)), "served_p99_ms": float(np.percentile(lat, 99)),
+            "plain_jobs_per_s": len(stream) / t_plain, "plain_p50_ms": float(np.percentile(lat_plain, 50)),
+            "plain_p99_ms": float(np.percentile(lat_plain, 99)), "speedup_jobs_per_s": t_plain / t_served,
+            "batches": st["batches"], "max_batch_jobs": st["max_batch_jobs"], "host_threads": cores,
+            "identical_to_plain": bool(same)}
+
+
 def run_ours(args, wl, rank, world, dist):
     import ctypes
 
@@ -393,6 +453,8 @@ def run_ours(args, wl, rank, world, dist):
     }
     if not args.no_batch:
         line["batch"] = run_batch_section(ctx)
+    if args.serve_jobs > 0:
+        line["serve"] = run_serve_section(ctx, args.serve_jobs, args.serve_nmax)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(wl)
     if rank == 0:
@@ -409,6 +471,8 @@ def main():
     ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-clusters section")
+    ap.add_argument("--serve-jobs", type=int, default=200, help="jobs in the serving section (0 = skip)")
+    ap.add_argument("--serve-nmax", type=int, default=50000, help="largest job (candidates) in the serving stream")
     ap.add_argument("--subset", type=int, default=0,
                     help="use a seeded random subset of this many words (profiling runs)")
     args = ap.parse_args()

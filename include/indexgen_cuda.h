@@ -141,6 +141,46 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
                          const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
                          int32_t *order, int32_t *counts, int64_t *edges);
 
+/* ---- serving: continuous batching of codebook jobs --------------------- */
+/* A server owns a scheduler thread and a pool of greedy threads on top of a
+ * context.  Jobs of any (n, len, min_ed) are submitted from any thread; the
+ * scheduler admits the jobs that have arrived, in arrival order, while the
+ * batch stays within hbm_budget_bytes (estimated footprint) and
+ * max_batch_pairs, builds them with one device pipeline, and admits the next
+ * arrivals while the greedy threads finish the previous batch.  A job's
+ * codebook is the same as ig_solve's for it alone.  There is no counterpart
+ * in the reference, which solves one job per program run. */
+typedef struct ig_server ig_server;
+typedef struct ig_server_opts {
+    int host_threads;          /* greedy threads (0 = all cores)                  */
+    int max_batch_jobs;        /* jobs per launch (0 = 256)                       */
+    int order_threads;         /* neighbour order (0 or 1 = canonical sorted)     */
+    int reserved;
+    int64_t max_batch_pairs;   /* pair tests per launch (0 = 2e10, ~0.1 s)        */
+    int64_t hbm_budget_bytes;  /* estimated HBM per launch (0 = half the free HBM) */
+} ig_server_opts;
+/* Job states reported by ig_server_poll. */
+#define IG_JOB_QUEUED 0
+#define IG_JOB_ON_DEVICE 1
+#define IG_JOB_GREEDY 2
+#define IG_JOB_DONE 3
+#define IG_JOB_CANCELLED 4
+#define IG_JOB_FAILED 5
+ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **out);
+/* Copies the words; returns at once with a ticket. */
+ig_status ig_server_submit(ig_server *sv, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *ticket);
+ig_status ig_server_poll(ig_server *sv, int64_t ticket, int *state);
+/* Blocks until the job is done; writes its codebook (order[n] job-local ids in
+ * selection order), size, edge count and submit-to-done latency, then forgets
+ * the ticket.  IG_ERR_CANCELLED / the failure status otherwise. */
+ig_status ig_server_wait(ig_server *sv, int64_t ticket, int32_t *order, int32_t *count, int64_t *edges,
+                         double *latency_ms);
+/* Cancels a job that is still queued (IG_ERR_STATE once it has started). */
+ig_status ig_server_cancel(ig_server *sv, int64_t ticket);
+ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, int64_t *max_batch_jobs);
+/* Cancels queued jobs, finishes the running batch, joins the threads. */
+ig_status ig_server_destroy(ig_server *sv);
+
 /* ---- one-call conveniences --------------------------------------------- */
 
 /* SolveIndependentSet (src/SparseMat.cpp:784-851): graph + greedy.

@@ -9,6 +9,7 @@ from .graph import (  # noqa: F401
     ConflictGraph,
     Context,
     IndexGenError,
+    Server,
     apply_filters,
     build_batch,
     build_conflict_graph,

@@ -21,6 +21,8 @@ EXPORTS = (
     "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
     "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_codebooks", "ig_solve_batch",
+    "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
+    "ig_server_stats", "ig_server_destroy",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -35,6 +37,15 @@ class IndexGenError(RuntimeError):
 
 
 _lib = None
+
+
+class ServerOpts(ctypes.Structure):
+    """ig_server_opts of include/indexgen_cuda.h."""
+
+    _fields_ = [("host_threads", ctypes.c_int), ("max_batch_jobs", ctypes.c_int), ("order_threads", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("max_batch_pairs", ctypes.c_int64),
+                ("hbm_budget_bytes", ctypes.c_int64)]
+
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -74,6 +85,14 @@ def _declare(L):
         "ig_graph_job_stats": (_int, [_vp, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
         "ig_graph_job_codebooks": (_int, [_vp, _int, _int, _vp, _vp]),
         "ig_solve_batch": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, _int, _vp, _vp, _vp]),
+        "ig_server_create": (_int, [_vp, ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)]),
+        "ig_server_submit": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),
+        "ig_server_poll": (_int, [_vp, _i64, ctypes.POINTER(_int)]),
+        "ig_server_wait": (_int, [_vp, _i64, _vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64),
+                                  ctypes.POINTER(ctypes.c_double)]),
+        "ig_server_cancel": (_int, [_vp, _i64]),
+        "ig_server_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+        "ig_server_destroy": (_int, [_vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -2,6 +2,7 @@
 // include/indexgen_cuda.h).
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -10,10 +11,6 @@
 
 #include "ig_internal.h"
 
-struct ig_ctx : ig::Ctx {
-};
-struct ig_graph : ig::Graph {
-};
 
 namespace ig {
 
@@ -154,60 +151,6 @@ ig_status fetch_adjacency(ig_graph *g, std::vector<int64_t> &ap, std::vector<int
     return IG_OK;
 }
 
-// Greedy of every job of a graph on `host_threads` host threads, largest job
-// first.  Job j's selection (job-local ids) goes to order + word_off_j.
-ig_status job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
-{
-    std::vector<int64_t> ap;
-    std::vector<int32_t> adj;
-    ig_status s = order_threads == 1 ? fetch_adjacency(g, ap, adj) : fetch_host(g);
-    if (s != IG_OK)
-        return s;
-    const int k = (int)g->jobs.size();
-    std::vector<int> seq((size_t)k);
-    std::iota(seq.begin(), seq.end(), 0);
-    std::stable_sort(seq.begin(), seq.end(), [&](int a, int b) {
-        return g->job_edge_off[(size_t)a + 1] - g->job_edge_off[(size_t)a] >
-               g->job_edge_off[(size_t)b + 1] - g->job_edge_off[(size_t)b];
-    });
-    std::atomic<int> next{0};
-    std::atomic<bool> failed{false};
-    auto worker = [&]() {
-        for (;;) {
-            const int q = next++;
-            if (q >= k)
-                return;
-            const JobSpec &J = g->jobs[(size_t)seq[(size_t)q]];
-            try {
-                int32_t c;
-                if (order_threads == 1)
-                    c = greedy_from_adjacency(ap.data() + J.word_off, adj.data(), J.n, J.word_off,
-                                              order + J.word_off);
-                else
-                    c = greedy_from_upper(g->h_row_ptr.data() + J.word_off, g->h_cols.data(), J.n, J.word_off,
-                                          order_threads, order + J.word_off);
-                counts[seq[(size_t)q]] = c;
-            } catch (...) {
-                failed = true;
-            }
-        }
-    };
-    int T = host_threads > 0 ? host_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-    T = std::max(1, std::min(T, k));
-    if (T == 1) {
-        worker();
-    } else {
-        std::vector<std::thread> pool;
-        for (int t = 0; t < T; ++t)
-            pool.emplace_back(worker);
-        for (auto &th : pool)
-            th.join();
-    }
-    if (failed)
-        return set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
-    return IG_OK;
-}
-
 // Validated job list from an offsets array.
 ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *lens, const int32_t *min_eds,
                     std::vector<JobSpec> &jobs)
@@ -225,6 +168,89 @@ ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *
     }
     if (k > 0 && offsets[k] > INT32_MAX)
         return set_error(ctx, IG_ERR_CAPACITY, "more than 2^31-1 words in one batch");
+    return IG_OK;
+}
+
+}  // namespace
+
+// What the host greedy needs of a graph, downloaded once: the canonical
+// adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
+
+ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
+{
+    ig_graph *g = static_cast<ig_graph *>(gg);
+    hg.order_threads = order_threads;
+    hg.jobs = g->jobs;
+    hg.job_edge_off = g->job_edge_off;
+    if (order_threads == 1)
+        return fetch_adjacency(g, hg.ptr, hg.idx);
+    ig_status s = fetch_host(g);
+    if (s == IG_OK) {
+        hg.ptr = g->h_row_ptr;
+        hg.idx = g->h_cols;
+    }
+    return s;
+}
+
+// Greedy of every job on `host_threads` host threads (pure host work),
+// largest job first.  Job j's selection (job-local ids) goes to
+// order + word_off_j - order_base; counts[j] its size.
+int32_t greedy_one(const HostGraph &hg, int job, int32_t *out)
+{
+    const JobSpec &J = hg.jobs[(size_t)job];
+    if (hg.order_threads == 1)
+        return greedy_from_adjacency(hg.ptr.data() + J.word_off, hg.idx.data(), J.n, J.word_off, out);
+    return greedy_from_upper(hg.ptr.data() + J.word_off, hg.idx.data(), J.n, J.word_off, hg.order_threads, out);
+}
+
+bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts)
+{
+    const int k = (int)hg.jobs.size();
+    std::vector<int> seq((size_t)k);
+    std::iota(seq.begin(), seq.end(), 0);
+    std::stable_sort(seq.begin(), seq.end(), [&](int a, int b) {
+        return hg.job_edge_off[(size_t)a + 1] - hg.job_edge_off[(size_t)a] >
+               hg.job_edge_off[(size_t)b + 1] - hg.job_edge_off[(size_t)b];
+    });
+    std::atomic<int> next{0};
+    std::atomic<bool> failed{false};
+    auto worker = [&]() {
+        for (;;) {
+            const int q = next++;
+            if (q >= k)
+                return;
+            const JobSpec &J = hg.jobs[(size_t)seq[(size_t)q]];
+            try {
+                counts[seq[(size_t)q]] = greedy_one(hg, seq[(size_t)q], order + (J.word_off - order_base));
+            } catch (...) {
+                failed = true;
+            }
+        }
+    };
+    int T = host_threads > 0 ? host_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    T = std::max(1, std::min(T, k));
+    if (T == 1) {
+        worker();
+    } else {
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; ++t)
+            pool.emplace_back(worker);
+        for (auto &th : pool)
+            th.join();
+    }
+    return !failed;
+}
+
+namespace {
+
+ig_status job_codebooks_impl(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
+{
+    HostGraph hg;
+    ig_status s = download_for_greedy(g, order_threads, hg);
+    if (s != IG_OK)
+        return s;
+    if (!run_greedies(hg, host_threads, 0, order, counts))
+        return set_error(g->ctx, IG_ERR_OOM, "host greedy allocation failed");
     return IG_OK;
 }
 
@@ -514,7 +540,7 @@ ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int3
     if (g->jobs.size() != 1)
         return ig::set_error(g->ctx, IG_ERR_STATE, "graph holds several jobs: use ig_graph_job_codebooks");
     int32_t c = 0;
-    ig_status s = ig::job_codebooks(g, order_threads, 1, order, &c);
+    ig_status s = ig::job_codebooks_impl(g, order_threads, 1, order, &c);
     if (s == IG_OK)
         *count = c;
     return s;
@@ -545,7 +571,7 @@ ig_status ig_graph_job_codebooks(ig_graph *g, int order_threads, int host_thread
 {
     if (!g || order_threads < 1 || (g->n > 0 && !order) || (!g->jobs.empty() && !counts))
         return IG_ERR_INPUT;
-    return ig::job_codebooks(g, order_threads, host_threads, order, counts);
+    return ig::job_codebooks_impl(g, order_threads, host_threads, order, counts);
 }
 
 ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
@@ -586,15 +612,57 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
 {
     if (!ctx || order_threads < 1 || (jobs > 0 && (!order || !counts)))
         return IG_ERR_INPUT;
-    ig_graph *g = nullptr;
-    ig_status s = ig_batch_build(ctx, words, offsets, jobs, lens, min_eds, 0, &g);
+    std::vector<ig::JobSpec> spec;
+    ig_status s = ig::make_jobs(ctx, offsets, jobs, lens, min_eds, spec);
     if (s != IG_OK)
         return s;
-    if (edges)
-        for (int32_t j = 0; j < jobs; ++j)
-            edges[j] = g->job_edge_off[(size_t)j + 1] - g->job_edge_off[(size_t)j];
-    s = ig::job_codebooks(g, order_threads, host_threads, order, counts);
-    ig::release_graph(g);
+    // Pipeline: the batch is cut into up to four contiguous groups of about
+    // equal pair count; while the device builds group g+1, host threads run
+    // the greedies of group g.
+    long double total = 0;
+    for (const ig::JobSpec &j : spec)
+        total += (long double)j.n * j.n;
+    const int groups = std::max(1, std::min<int>(4, jobs));
+    std::vector<int> cut{0};
+    long double acc = 0;
+    for (int32_t j = 0; j < jobs; ++j) {
+        acc += (long double)spec[(size_t)j].n * spec[(size_t)j].n;
+        if ((int)cut.size() < groups && acc >= total * cut.size() / groups && j + 1 < jobs)
+            cut.push_back(j + 1);
+    }
+    cut.push_back(jobs);
+    std::thread host;
+    bool host_ok = true;
+    for (size_t gi = 0; gi + 1 < cut.size(); ++gi) {
+        const int lo = cut[gi], hi = cut[gi + 1];
+        if (lo >= hi)
+            continue;
+        std::vector<int64_t> sub((size_t)(hi - lo) + 1);
+        for (int j = lo; j <= hi; ++j)
+            sub[(size_t)(j - lo)] = offsets[j] - offsets[lo];
+        ig_graph *g = nullptr;
+        s = ig_batch_build(ctx, words + offsets[lo], sub.data(), hi - lo, lens + lo, min_eds + lo, 0, &g);
+        if (s != IG_OK)
+            break;
+        if (edges)
+            for (int j = lo; j < hi; ++j)
+                edges[j] = g->job_edge_off[(size_t)(j - lo) + 1] - g->job_edge_off[(size_t)(j - lo)];
+        auto hg = std::make_shared<ig::HostGraph>();
+        s = ig::download_for_greedy(g, order_threads, *hg);
+        ig::release_graph(g);
+        if (s != IG_OK)
+            break;
+        if (host.joinable())
+            host.join();
+        host = std::thread([hg, host_threads, order, counts, lo, off = offsets[lo], &host_ok]() {
+            if (!ig::run_greedies(*hg, host_threads, 0, order + off, counts + lo))
+                host_ok = false;
+        });
+    }
+    if (host.joinable())
+        host.join();
+    if (s == IG_OK && !host_ok)
+        s = ig::set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
     return s;
 }
 

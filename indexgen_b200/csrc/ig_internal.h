@@ -122,7 +122,30 @@ int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n
 int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int64_t base,
                               int32_t *order);
 
+// What the host greedy needs of a graph, downloaded once: the canonical
+// adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
+struct HostGraph {
+    int order_threads = 1;
+    std::vector<int64_t> ptr;  // adjacency or row offsets, [n+1]
+    std::vector<int32_t> idx;  // neighbour / column ids (global)
+    std::vector<JobSpec> jobs;
+    std::vector<int64_t> job_edge_off;
+};
+// Device -> host (ig_api.cu); the graph stays valid.
+ig_status download_for_greedy(Graph *g, int order_threads, HostGraph &hg);
+// Greedy of every job on host threads, largest first; job j's selection goes
+// to order + word_off_j - order_base.  False on allocation failure.
+bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts);
+// Greedy of one job of a downloaded graph into out (job-local ids).
+int32_t greedy_one(const HostGraph &hg, int job, int32_t *out);
+
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);
 
 }  // namespace ig
+
+// The opaque ABI handles are the internal objects.
+struct ig_ctx : ig::Ctx {
+};
+struct ig_graph : ig::Graph {
+};

@@ -1,0 +1,375 @@
+// Serving loop: continuous batching of codebook jobs of mixed (n, L, d).
+//
+// The reference solves one job per process invocation (src/SparseMat.cpp:878)
+// and, in the clustered mode, one python3 GPU process per cluster
+// (src/SparseMat.cpp:805-814).  Here a long-lived server owns a context and
+// two stages that overlap:
+//   scheduler thread  takes the jobs that have arrived, in arrival order, as
+//                     long as the batch stays within the HBM budget (footprint
+//                     estimated per job) and the per-launch pair budget; builds
+//                     all their graphs with one device pipeline (one persistent
+//                     pair-test launch); downloads the canonical adjacency; hands
+//                     the jobs to the greedy pool; and immediately admits the
+//                     jobs that arrived meanwhile.
+//   greedy pool       host threads run each job's greedy while the device works
+//                     on the next batch; a job is done when its greedy is.
+// A job's result does not depend on what it was batched with: its graph is a
+// diagonal block of the batch graph and its greedy runs on that block alone.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <new>
+#include <thread>
+#include <unordered_map>
+
+#include "ig_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+enum JobState { kQueued = 0, kOnDevice = 1, kGreedy = 2, kDone = 3, kCancelled = 4, kFailed = 5 };
+
+struct ServerJob {
+    int64_t ticket = 0;
+    std::vector<uint32_t> words;
+    int32_t n = 0, len = 1, min_ed = 0;
+    int64_t footprint = 0;
+    long double pairs = 0;
+    JobState state = kQueued;
+    ig_status status = IG_OK;
+    Clock::time_point t_submit, t_done;
+    std::vector<int32_t> order;
+    int32_t count = 0;
+    int64_t edges = 0;
+};
+
+struct GreedyTask {
+    std::shared_ptr<ig::HostGraph> hg;
+    int job_in_batch = 0;
+    std::shared_ptr<ServerJob> job;
+};
+
+// Edge density P(ED < d) of filtered uniform strings, per (n, d), used only to
+// estimate how much HBM a job will need before its pairs are counted.
+double density_estimate(int len, int min_ed)
+{
+    static const double tab[7][3] = {{6.3e-4, 6.8e-3, 4.6e-2}, {2.1e-4, 2.7e-3, 2.0e-2}, {5.0e-5, 8.3e-4, 7.5e-3},
+                                     {1.5e-5, 2.5e-4, 2.7e-3}, {5e-6, 1.0e-4, 1.0e-3},   {5e-6, 2.0e-5, 3.7e-4},
+                                     {5e-6, 5e-6, 1.2e-4}};
+    if (min_ed <= 0)
+        return 0.0;
+    if (len >= 10 && len <= 16 && min_ed >= 3 && min_ed <= 5)
+        return tab[len - 10][min_ed - 3];
+    return min_ed > len ? 1.0 : 0.05;  // outside the table: be generous
+}
+
+int64_t footprint_estimate(int32_t n, int len, int min_ed)
+{
+    const long double pairs = (long double)n * (n > 0 ? n - 1 : 0) / 2;
+    const long double edges = std::min<long double>(pairs, pairs * density_estimate(len, min_ed) * 2 + 1024);
+    const long double nseg = std::min<long double>(256, std::max<long double>(1, n / 256.0));
+    // words + units + segment counts + CSR offsets + records + columns + adjacency
+    return (int64_t)(4.0L * n + 32.0L * n + 4.0L * n * nseg + 16.0L * n + 16 * edges + 4 * edges + 8 * edges);
+}
+
+}  // namespace
+
+struct ig_server {
+    ig_ctx *ctx = nullptr;
+    ig_server_opts opts{};
+    std::mutex mu;
+    std::condition_variable cv_queue, cv_done, cv_tasks;
+    std::deque<std::shared_ptr<ServerJob>> queue;
+    std::unordered_map<int64_t, std::shared_ptr<ServerJob>> jobs;
+    std::deque<GreedyTask> tasks;
+    int64_t next_ticket = 1;
+    bool stopping = false;
+    bool scheduler_done = false;
+    std::thread scheduler;
+    std::vector<std::thread> pool;
+    // counters
+    int64_t batches = 0, completed = 0, failed = 0, cancelled = 0, max_batch = 0;
+
+    void schedule_loop();
+    void greedy_loop();
+};
+
+void ig_server::schedule_loop()
+{
+    for (;;) {
+        std::vector<std::shared_ptr<ServerJob>> batch;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_queue.wait(lk, [&] { return stopping || !queue.empty(); });
+            if (stopping && queue.empty())
+                return;
+            int64_t mem = 0;
+            long double pairs = 0;
+            while (!queue.empty()) {
+                std::shared_ptr<ServerJob> j = queue.front();
+                if (j->state == kCancelled) {
+                    queue.pop_front();
+                    continue;
+                }
+                const bool first = batch.empty();
+                if (!first && ((int)batch.size() >= opts.max_batch_jobs || mem + j->footprint > opts.hbm_budget_bytes ||
+                               pairs + j->pairs > (long double)opts.max_batch_pairs))
+                    break;
+                queue.pop_front();
+                j->state = kOnDevice;
+                mem += j->footprint;
+                pairs += j->pairs;
+                batch.push_back(j);
+            }
+        }
+        if (batch.empty())
+            continue;
+        // one device pipeline for the whole batch
+        std::vector<uint32_t> words;
+        std::vector<int64_t> off{0};
+        std::vector<int32_t> lens, eds;
+        for (auto &j : batch) {
+            words.insert(words.end(), j->words.begin(), j->words.end());
+            off.push_back(off.back() + j->n);
+            lens.push_back(j->len);
+            eds.push_back(j->min_ed);
+        }
+        ig_graph *g = nullptr;
+        ig_status s = ig_batch_build(ctx, words.data(), off.data(), (int32_t)batch.size(), lens.data(), eds.data(), 0,
+                                     &g);
+        auto hg = std::make_shared<ig::HostGraph>();
+        if (s == IG_OK) {
+            s = ig::download_for_greedy(g, opts.order_threads, *hg);
+            ig_graph_free(g);
+        }
+        std::unique_lock<std::mutex> lk(mu);
+        ++batches;
+        max_batch = std::max<int64_t>(max_batch, (int64_t)batch.size());
+        if (s != IG_OK) {
+            for (auto &j : batch) {
+                j->state = kFailed;
+                j->status = s;
+                j->t_done = Clock::now();
+                ++failed;
+            }
+            cv_done.notify_all();
+            continue;
+        }
+        for (size_t b = 0; b < batch.size(); ++b) {
+            batch[b]->edges = hg->job_edge_off[b + 1] - hg->job_edge_off[b];
+            batch[b]->state = kGreedy;
+            tasks.push_back(GreedyTask{hg, (int)b, batch[b]});
+        }
+        cv_tasks.notify_all();
+    }
+}
+
+void ig_server::greedy_loop()
+{
+    for (;;) {
+        GreedyTask t;
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_tasks.wait(lk, [&] { return scheduler_done || !tasks.empty(); });
+            if (tasks.empty())
+                return;  // the scheduler has stopped and nothing is left
+            t = std::move(tasks.front());
+            tasks.pop_front();
+        }
+        ig_status s = IG_OK;
+        int32_t c = 0;
+        try {
+            t.job->order.resize((size_t)std::max(t.job->n, 1));
+            c = ig::greedy_one(*t.hg, t.job_in_batch, t.job->order.data());
+        } catch (...) {
+            s = IG_ERR_OOM;
+        }
+        t.hg.reset();
+        std::unique_lock<std::mutex> lk(mu);
+        t.job->count = c;
+        t.job->order.resize((size_t)c);
+        t.job->status = s;
+        t.job->state = s == IG_OK ? kDone : kFailed;
+        t.job->t_done = Clock::now();
+        if (s == IG_OK)
+            ++completed;
+        else
+            ++failed;
+        cv_done.notify_all();
+    }
+}
+
+extern "C" {
+
+ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **out)
+{
+    if (!ctx || !out)
+        return IG_ERR_INPUT;
+    *out = nullptr;
+    ig_server *sv = new (std::nothrow) ig_server();
+    if (!sv)
+        return IG_ERR_OOM;
+    sv->ctx = ctx;
+    ig_server_opts o{};
+    if (opts)
+        o = *opts;
+    if (o.host_threads <= 0)
+        o.host_threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (o.max_batch_jobs <= 0)
+        o.max_batch_jobs = 256;
+    if (o.max_batch_pairs <= 0)
+        o.max_batch_pairs = 20000000000ll;  // ~0.1 s of device work per launch
+    if (o.order_threads <= 0)
+        o.order_threads = 1;
+    if (o.hbm_budget_bytes <= 0) {
+        size_t free_b = 0, total_b = 0;
+        int prev = -1;
+        cudaGetDevice(&prev);
+        cudaSetDevice(ctx->device);
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+            free_b = (size_t)8 << 30;
+        cudaGetLastError();
+        if (prev >= 0)
+            cudaSetDevice(prev);
+        o.hbm_budget_bytes = (int64_t)(free_b / 2);
+    }
+    sv->opts = o;
+    sv->scheduler = std::thread([sv] { sv->schedule_loop(); });
+    for (int i = 0; i < o.host_threads; ++i)
+        sv->pool.emplace_back([sv] { sv->greedy_loop(); });
+    *out = sv;
+    return IG_OK;
+}
+
+ig_status ig_server_submit(ig_server *sv, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *ticket)
+{
+    if (!sv || !ticket || n < 0 || len < 1 || len > IG_MAX_LEN || (n > 0 && !words))
+        return IG_ERR_INPUT;
+    auto j = std::make_shared<ServerJob>();
+    try {
+        j->words.assign(words, words + n);
+    } catch (...) {
+        return IG_ERR_OOM;
+    }
+    j->n = n;
+    j->len = len;
+    j->min_ed = min_ed;
+    j->pairs = (long double)n * (n > 0 ? n - 1 : 0) / 2;
+    j->footprint = footprint_estimate(n, len, min_ed);
+    j->t_submit = Clock::now();
+    std::unique_lock<std::mutex> lk(sv->mu);
+    if (sv->stopping)
+        return IG_ERR_STATE;
+    j->ticket = sv->next_ticket++;
+    sv->jobs[j->ticket] = j;
+    sv->queue.push_back(j);
+    *ticket = j->ticket;
+    sv->cv_queue.notify_one();
+    return IG_OK;
+}
+
+ig_status ig_server_poll(ig_server *sv, int64_t ticket, int *state)
+{
+    if (!sv || !state)
+        return IG_ERR_INPUT;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(ticket);
+    if (it == sv->jobs.end())
+        return IG_ERR_INPUT;
+    *state = (int)it->second->state;
+    return IG_OK;
+}
+
+ig_status ig_server_wait(ig_server *sv, int64_t ticket, int32_t *order, int32_t *count, int64_t *edges,
+                         double *latency_ms)
+{
+    if (!sv || !count)
+        return IG_ERR_INPUT;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(ticket);
+    if (it == sv->jobs.end())
+        return IG_ERR_INPUT;
+    std::shared_ptr<ServerJob> j = it->second;
+    sv->cv_done.wait(lk, [&] { return j->state >= kDone; });
+    sv->jobs.erase(it);
+    if (latency_ms)
+        *latency_ms = std::chrono::duration<double, std::milli>(j->t_done - j->t_submit).count();
+    if (j->state == kCancelled)
+        return IG_ERR_CANCELLED;
+    if (j->state == kFailed)
+        return j->status;
+    if (j->count > 0 && !order)
+        return IG_ERR_INPUT;
+    if (j->count > 0)
+        std::copy(j->order.begin(), j->order.end(), order);
+    *count = j->count;
+    if (edges)
+        *edges = j->edges;
+    return IG_OK;
+}
+
+ig_status ig_server_cancel(ig_server *sv, int64_t ticket)
+{
+    if (!sv)
+        return IG_ERR_INPUT;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->jobs.find(ticket);
+    if (it == sv->jobs.end())
+        return IG_ERR_INPUT;
+    if (it->second->state != kQueued)
+        return IG_ERR_STATE;  // already on the device or finished
+    it->second->state = kCancelled;
+    it->second->t_done = Clock::now();
+    ++sv->cancelled;
+    sv->cv_done.notify_all();
+    return IG_OK;
+}
+
+ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, int64_t *max_batch_jobs)
+{
+    if (!sv)
+        return IG_ERR_INPUT;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    if (batches)
+        *batches = sv->batches;
+    if (completed)
+        *completed = sv->completed;
+    if (max_batch_jobs)
+        *max_batch_jobs = sv->max_batch;
+    return IG_OK;
+}
+
+ig_status ig_server_destroy(ig_server *sv)
+{
+    if (!sv)
+        return IG_ERR_INPUT;
+    {
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->stopping = true;
+        for (auto &j : sv->queue)
+            if (j->state == kQueued) {
+                j->state = kCancelled;
+                j->t_done = Clock::now();
+            }
+        sv->queue.clear();
+        sv->cv_queue.notify_all();
+        sv->cv_tasks.notify_all();
+        sv->cv_done.notify_all();
+    }
+    if (sv->scheduler.joinable())
+        sv->scheduler.join();
+    {
+        std::unique_lock<std::mutex> lk(sv->mu);
+        sv->scheduler_done = true;
+        sv->cv_tasks.notify_all();
+    }
+    for (auto &t : sv->pool)
+        t.join();
+    delete sv;
+    return IG_OK;
+}
+
+}  // extern "C"

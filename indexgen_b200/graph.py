@@ -281,6 +281,81 @@ def solve(words, L: int, min_ed: int, order_threads: int = 1, ctx: Context | Non
     return order[: cnt.value], int(e.value)
 
 
+class Server:
+    """Continuous-batching codebook server (ig_server_*): submit jobs from any
+    thread, wait for their codebooks.  Each result equals solve() of the job
+    alone."""
+
+    STATES = ("queued", "on_device", "greedy", "done", "cancelled", "failed")
+
+    def __init__(self, ctx: Context | None = None, host_threads: int = 0, max_batch_jobs: int = 0,
+                 max_batch_pairs: int = 0, hbm_budget_bytes: int = 0, order_threads: int = 1):
+        self.ctx = ctx or default_context()
+        o = _lib.ServerOpts(host_threads, max_batch_jobs, order_threads, 0, max_batch_pairs, hbm_budget_bytes)
+        h = ctypes.c_void_p()
+        check(lib().ig_server_create(self.ctx.handle, ctypes.byref(o), ctypes.byref(h)), "ig_server_create",
+              self.ctx.handle)
+        self.handle = h
+        self._n = {}
+
+    def submit(self, words, L: int, min_ed: int) -> int:
+        w = _words_array(words)
+        t = ctypes.c_int64()
+        check(lib().ig_server_submit(self.handle, ptr(w), len(w), int(L), int(min_ed), ctypes.byref(t)),
+              "ig_server_submit")
+        self._n[t.value] = len(w)
+        return int(t.value)
+
+    def poll(self, ticket: int) -> str:
+        st = ctypes.c_int()
+        check(lib().ig_server_poll(self.handle, int(ticket), ctypes.byref(st)), "ig_server_poll")
+        return self.STATES[st.value]
+
+    def wait(self, ticket: int):
+        """(codebook ids in selection order, edges, latency_ms)."""
+        n = self._n.pop(ticket, 0)
+        order = np.zeros(max(n, 1), np.int32)
+        cnt = ctypes.c_int32()
+        e = ctypes.c_int64()
+        lat = ctypes.c_double()
+        check(lib().ig_server_wait(self.handle, int(ticket), ptr(order), ctypes.byref(cnt), ctypes.byref(e),
+                                   ctypes.byref(lat)), "ig_server_wait")
+        return order[: cnt.value].copy(), int(e.value), float(lat.value)
+
+    def cancel(self, ticket: int) -> bool:
+        """True if the job was still queued and is now cancelled."""
+        st = lib().ig_server_cancel(self.handle, int(ticket))
+        if st == 7:  # IG_ERR_STATE: already running
+            return False
+        check(st, "ig_server_cancel")
+        return True
+
+    def stats(self):
+        b = ctypes.c_int64()
+        c = ctypes.c_int64()
+        m = ctypes.c_int64()
+        check(lib().ig_server_stats(self.handle, ctypes.byref(b), ctypes.byref(c), ctypes.byref(m)),
+              "ig_server_stats")
+        return {"batches": int(b.value), "completed": int(c.value), "max_batch_jobs": int(m.value)}
+
+    def close(self):
+        if self.handle:
+            lib().ig_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 # ---------------------------------------------------------------------------
 # Reference-named entry points
 # ---------------------------------------------------------------------------
@@ -360,7 +435,7 @@ def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
 
 
 __all__ = [
-    "Context", "ConflictGraph", "IndexGenError", "build_conflict_graph", "build_batch", "solve_batch",
+    "Context", "ConflictGraph", "IndexGenError", "Server", "build_conflict_graph", "build_batch", "solve_batch",
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context",

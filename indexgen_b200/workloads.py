@@ -255,3 +255,22 @@ def clustered14(total: int = 1_000_000, k: int = 64, seed: int = 14):
     w = uniform_until(total, 14, seed, max_run=3, min_gc=0.3, max_gc=0.7)
     parts = assign_clusters(w, 14, zipf_sizes(total, k), seed + 1)
     return [w[p] for p in parts]
+
+
+def serving_stream(jobs: int, seed: int, rate: float = 50.0, nmin: int = 5000, nmax: int = 500000,
+                   lengths=(10, 16), dists=(3, 5)):
+    """Seeded stream of codebook jobs: Poisson arrivals (mean `rate` jobs/s),
+    n uniform in [lengths], editDist uniform in [dists], candidate count
+    log-uniform in [nmin, nmax] (counted after the maxRun 3 / GC [0.3,0.7]
+    filters).  Returns a list of (arrival_s, words, n, editDist)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(jobs):
+        t += rng.exponential(1.0 / rate)
+        L = int(rng.integers(lengths[0], lengths[1] + 1))
+        d = int(rng.integers(dists[0], dists[1] + 1))
+        count = int(round(float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))))
+        words = uniform_until(count, L, int(rng.integers(1 << 31)), max_run=3, min_gc=0.3, max_gc=0.7)
+        out.append((t, words, L, d))
+    return out
