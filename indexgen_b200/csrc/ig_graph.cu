@@ -34,6 +34,11 @@ namespace ig {
 
 namespace {
 
+using myers::BandConst;
+using myers::BandUnit;
+using myers::kModeByte;
+using myers::kModeFull;
+using myers::kModeNib;
 using myers::Unit;
 using myers::imad;
 using myers::myers_one;
@@ -145,6 +150,49 @@ __global__ void prep_units(const uint32_t *__restrict__ words, const JobDesc *__
     const long long p = u - J.unit_start;
     const uint32_t *w = words + J.word_off;
     uint4 *out = units + J.unit_off;
+    if (J.mode == kModeNib) {
+        // 8 columns; word j: columns 0,2,4,6 in bits 0..15, 1,3,5,7 in 16..31
+        uint32_t cw[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            cw[c] = (8 * p + c < J.n) ? w[8 * p + c] : 0u;
+        uint32_t o[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            uint32_t x = 0u;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                x |= ((cw[2 * m] >> (2 * j)) & 3u) << (4 * m);
+                x |= ((cw[2 * m + 1] >> (2 * j)) & 3u) << (16 + 4 * m);
+            }
+            o[j] = x;
+        }
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            out[4 * p + v] = make_uint4(o[4 * v], o[4 * v + 1], o[4 * v + 2], o[4 * v + 3]);
+        return;
+    }
+    if (J.mode == kModeByte) {
+        // 4 columns; word q: positions 2q (bits 0..15) and 2q+1 (16..31)
+        uint32_t cw[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            cw[c] = (4 * p + c < J.n) ? w[4 * p + c] : 0u;
+        uint32_t o[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            uint32_t x = 0u;
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                x |= ((cw[l] >> (4 * q)) & 3u) << (4 * l);
+                x |= ((cw[l] >> (4 * q + 2)) & 3u) << (16 + 4 * l);
+            }
+            o[q] = x;
+        }
+        out[2 * p] = make_uint4(o[0], o[1], o[2], o[3]);
+        out[2 * p + 1] = make_uint4(o[4], o[5], o[6], o[7]);
+        return;
+    }
     if (J.L <= 15) {
         const uint32_t wa = w[2 * p];
         const uint32_t wb = (2 * p + 1 < J.n) ? w[2 * p + 1] : wa;
@@ -172,9 +220,11 @@ struct PairArgs {
     const JobDesc *jobs;
     int njobs;
     long long items;
-    uint32_t one;     // 1 and 2 (and 1 << 16) as opaque operands for imad / umulhi
+    uint32_t one;     // 1, 2, 2^16, 2^28, 2^31 as opaque operands for imad / umulhi
     uint32_t two;
     uint32_t hi;
+    uint32_t h28;
+    uint32_t h31;
     unsigned long long *work;
     unsigned long long *rec_count;
     EdgeRecord *rec;
@@ -273,15 +323,83 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
     }
 }
 
-constexpr int kSlotVec = kTileCols * 2;  // uint4 per staged tile (8 KiB, both unit layouts)
+// Banded forms: one unit = 8 (kNib) or 4 (kByte) columns.
+template <int L, int MODE, bool CHECK>
+__device__ __forceinline__ void tile_pass_band(const PairArgs &a, const uint4 *tile, int nu, int32_t c0,
+                                               const RowCtx &r, const uint32_t (&W)[L], const BandConst &q,
+                                               uint32_t &rank, int lane)
+{
+    using BU = BandUnit<MODE>;
+    for (int u = 0; u < nu; ++u) {
+        const uint4 *src = tile + u * BU::kVec;
+        uint32_t he, ho;
+        if constexpr (MODE == kModeNib) {
+            uint32_t sel[16];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                if (4 * v < L) {
+                    const uint4 t4 = src[v];
+                    sel[4 * v] = t4.x;
+                    sel[4 * v + 1] = t4.y;
+                    sel[4 * v + 2] = t4.z;
+                    sel[4 * v + 3] = t4.w;
+                } else {
+                    sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
+                }
+            }
+            myers::band_nib<L>(W, sel, q, he, ho);
+        } else {
+            uint32_t sel[8];
+#pragma unroll
+            for (int v = 0; v < 2; ++v) {
+                if (8 * v < L) {
+                    const uint4 t4 = src[v];
+                    sel[4 * v] = t4.x;
+                    sel[4 * v + 1] = t4.y;
+                    sel[4 * v + 2] = t4.z;
+                    sel[4 * v + 3] = t4.w;
+                } else {
+                    sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
+                }
+            }
+            he = myers::band_byte<L>(W, sel, q);
+            ho = 0u;
+        }
+        if (__any_sync(kFull, (he | ho) != 0u)) {
+            const int32_t base_col = c0 + u * BU::kCols;
+#pragma unroll
+            for (int c = 0; c < BU::kCols; ++c) {
+                bool hit;
+                if (MODE == kModeNib)
+                    hit = (((c & 1) ? ho : he) >> (8 * (c >> 1) + 7)) & 1u;
+                else
+                    hit = (he >> (8 * c + 7)) & 1u;
+                const int32_t col = base_col + c;
+                if (CHECK)
+                    hit = hit && r.ok && (col > r.row) && (col < r.n);
+                emit_hit(a, hit, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
+            }
+        }
+    }
+}
+
+constexpr int kSlotVec = kTileCols * 2;  // uint4 per staged tile (8 KiB, every unit layout)
+
+// Column-unit geometry of a lane form.
+template <int L, int MODE>
+struct Geo {
+    static constexpr int kCols = MODE == kModeFull ? Unit<L>::kCols : BandUnit<MODE>::kCols;
+    static constexpr int kVec = MODE == kModeFull ? Unit<L>::kVec : BandUnit<MODE>::kVec;
+    static constexpr int kBytes = kVec * 16;
+};
 
 // One (band, segment) item of job J: stream the segment's column tiles through
 // the two-slot ring and test them against the band's rows.
-template <int L>
+template <int L, int MODE>
 __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, int band, int seg,
                                          uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity, bool &aborted)
 {
-    using U = Unit<L>;
+    using G = Geo<L, MODE>;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int32_t row0 = band * kBandRows;
@@ -293,13 +411,29 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     r.base = (uint32_t)J.word_off;
     r.grow = (uint32_t)(J.word_off + r.row);
     r.cell = (uint32_t)(J.count_off + (long long)seg * J.n + r.row);
-    row_pools<L>(a.words[J.word_off + (r.ok ? r.row : 0)], r.p01, r.p23);
+    const uint32_t rword = a.words[J.word_off + (r.ok ? r.row : 0)];
+    uint32_t W[MODE == kModeFull ? 1 : L];
+    BandConst q;
+    if constexpr (MODE == kModeFull) {
+        row_pools<L>(rword, r.p01, r.p23);
+    } else {
+        myers::band_windows<L, MODE>(rword, J.w, W);
+        q.vp0 = J.vp0;
+        q.bm = J.bm;
+        q.c = J.cmask;
+        q.k = J.kthr;
+        q.one = a.one;
+        q.h16 = a.hi;
+        q.h28 = a.h28;
+        q.h31 = a.h31;
+    }
     // c_lo is a multiple of 256 (segments and bands are), so units never
     // straddle a segment
     const int32_t c_lo = (int32_t)max((long long)seg << J.seg_shift, (long long)row0);
     const int32_t c_hi = (int32_t)min((long long)(seg + 1) << J.seg_shift, (long long)J.n);
     const long long row_end = (long long)row0 + kBandRows;
-    const bool check = ((long long)c_lo < row_end) || (row_end > (long long)J.n) || (U::kCols == 2 && (c_hi & 1));
+    const bool check = ((long long)c_lo < row_end) || (row_end > (long long)J.n) ||
+                       (G::kCols > 1 && (c_hi % G::kCols) != 0);
     const int ntiles = (c_hi - c_lo + kTileCols - 1) / kTileCols;
     const uint4 *units = a.units + J.unit_off;
     uint32_t rank = 0;
@@ -307,10 +441,10 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     if (tid == 0) {
         for (int t = 0; t < 2 && t < ntiles; ++t) {
             const int32_t c0 = c_lo + t * kTileCols;
-            const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
-            const uint32_t bytes = (uint32_t)nu * U::kBytes;
+            const int nu = (min(kTileCols, c_hi - c0) + G::kCols - 1) / G::kCols;
+            const uint32_t bytes = (uint32_t)nu * G::kBytes;
             mbar_arrive_expect_tx(&bar[t], bytes);
-            bulk_g2s(&tile[t][0], units + (size_t)(c0 / U::kCols) * U::kVec, bytes, &bar[t]);
+            bulk_g2s(&tile[t][0], units + (size_t)(c0 / G::kCols) * G::kVec, bytes, &bar[t]);
         }
     }
     for (int t = 0; t < ntiles; ++t) {
@@ -332,22 +466,42 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
             return;
         }
         const int32_t c0 = c_lo + t * kTileCols;
-        const int nu = (min(kTileCols, c_hi - c0) + U::kCols - 1) / U::kCols;
-        if (check)
-            tile_pass<L, true>(a, tile[b], nu, c0, r, rank, lane);
-        else
-            tile_pass<L, false>(a, tile[b], nu, c0, r, rank, lane);
+        const int nu = (min(kTileCols, c_hi - c0) + G::kCols - 1) / G::kCols;
+        if constexpr (MODE == kModeFull) {
+            if (check)
+                tile_pass<L, true>(a, tile[b], nu, c0, r, rank, lane);
+            else
+                tile_pass<L, false>(a, tile[b], nu, c0, r, rank, lane);
+        } else {
+            if (check)
+                tile_pass_band<L, MODE, true>(a, tile[b], nu, c0, r, W, q, rank, lane);
+            else
+                tile_pass_band<L, MODE, false>(a, tile[b], nu, c0, r, W, q, rank, lane);
+        }
         __syncthreads();
         if (tid == 0 && t + 2 < ntiles) {
             const int32_t cn = c_lo + (t + 2) * kTileCols;
-            const int nun = (min(kTileCols, c_hi - cn) + U::kCols - 1) / U::kCols;
-            const uint32_t bytes = (uint32_t)nun * U::kBytes;
+            const int nun = (min(kTileCols, c_hi - cn) + G::kCols - 1) / G::kCols;
+            const uint32_t bytes = (uint32_t)nun * G::kBytes;
             mbar_arrive_expect_tx(&bar[b], bytes);
-            bulk_g2s(&tile[b][0], units + (size_t)(cn / U::kCols) * U::kVec, bytes, &bar[b]);
+            bulk_g2s(&tile[b][0], units + (size_t)(cn / G::kCols) * G::kVec, bytes, &bar[b]);
         }
     }
     if (r.ok)
         a.counts[r.cell] = rank;
+}
+
+template <int L>
+__device__ __forceinline__ void dispatch_mode(int mode, const PairArgs &a, const JobDesc &J, int band, int seg,
+                                              uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
+                                              bool &aborted)
+{
+    if (mode == kModeNib)
+        run_item<L, kModeNib>(a, J, band, seg, tile, bar, parity, aborted);
+    else if (mode == kModeByte)
+        run_item<L, kModeByte>(a, J, band, seg, tile, bar, parity, aborted);
+    else
+        run_item<L, kModeFull>(a, J, band, seg, tile, bar, parity, aborted);
 }
 
 template <int... Ls>
@@ -355,7 +509,7 @@ __device__ __forceinline__ void dispatch_item(int L, const PairArgs &a, const Jo
                                               uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
                                               bool &aborted, std::integer_sequence<int, Ls...>)
 {
-    ((L == Ls + 1 ? run_item<Ls + 1>(a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
+    ((L == Ls + 1 ? dispatch_mode<Ls + 1>(J.mode, a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
 }
 
 __global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
@@ -612,11 +766,34 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
         d.unit_start = out.units;
         d.unit_off = out.unit_vec;
         d.count_off = out.counts;
-        const long long units = j.len <= 15 ? ((long long)j.n + 1) / 2 : (long long)j.n;
-        out.items += j.n >= 2 ? p.items : 0;
+        d.mode = myers::band_mode(j.len, j.min_ed);
+        d.w = 0;
+        d.vp0 = d.bm = d.cmask = d.kthr = 0;
+        if (d.mode != kModeFull)
+            myers::band_constants(j.len, j.min_ed, d.mode, d.w, d.vp0, d.bm, d.cmask, d.kthr);
+        long long units, vec;
+        if (d.mode == kModeNib) {
+            units = ((long long)j.n + 7) / 8;
+            vec = 4;
+        } else if (d.mode == kModeByte) {
+            units = ((long long)j.n + 3) / 4;
+            vec = 2;
+        } else if (j.len <= 15) {
+            units = ((long long)j.n + 1) / 2;
+            vec = 4;
+        } else {
+            units = (long long)j.n;
+            vec = 2;
+        }
+        // n < 2 or min_ed <= 0: no pair can be an edge.  The job gets no items
+        // and no segments, so its rows read no count cells (degree 0).
+        const bool active = j.n >= 2 && j.min_ed >= 1;
+        if (!active)
+            d.nseg = 0;
+        out.items += active ? p.items : 0;
         out.units += units;
-        out.unit_vec += units * (j.len <= 15 ? 4 : 2);
-        out.counts += (long long)p.nseg * j.n;
+        out.unit_vec += units * vec;
+        out.counts += (long long)d.nseg * j.n;
         out.rows = std::max<int64_t>(out.rows, j.word_off + j.n);
         out.desc.push_back(d);
     }
@@ -660,6 +837,8 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.one = 1u;
     a.two = 2u;
     a.hi = 1u << 16;
+    a.h28 = 1u << 28;
+    a.h31 = 1u << 31;
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);

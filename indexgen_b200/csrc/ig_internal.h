@@ -33,7 +33,8 @@ struct JobDesc {
     int64_t count_off;   // first per-(segment, row) count ([nseg][n] block)
     int32_t n, L, lim;   // words, length, min_ed - L
     int32_t seg_shift, nseg, bands_per_seg, nbands;
-    int32_t pad;
+    int32_t mode, w;     // lane form (full Myers / banded nibble / banded byte), band half-width
+    uint32_t vp0, bm, cmask, kthr;  // banded-mode constants
 };
 
 // Host description of a job.

@@ -133,5 +133,156 @@ __device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint
     return (__popc(pv & M) - __popc(mv & M)) < lim;
 }
 
+// ---------------------------------------------------------------------------
+// Banded lanes.  For a threshold k = min_ed - 1 the decision ED <= k between
+// two equal-length strings only needs the diagonals |i - j| <= w, w = k/2
+// (Ukkonen): a path that leaves them costs more than k.  Each column's band is
+// a (2w+1)-bit vector, bit b <-> row i = j - w + b, and the recurrence is
+// Myers' with the band re-aligned by one row per column:
+//   D0 = (((Eq & VP) + VP) ^ VP) | Eq | VN          (carry out of the band dropped)
+//   HN = VP & D0;  HP = VN | ~(D0 | VP)
+//   Y  = D0 >> 1                                     (next column's alignment; 0 enters at the bottom)
+//   VN = Y & HP;   VP = HN | ~(Y | HP)
+// starting from VP = 1 on the band rows i >= 1 (rows <= 0 carry no delta) and
+// VN = 0.  The centre bit b = w is the main diagonal: D[L][L] = L - sum_j D0_j[w].
+// Many pair tests share one 32-bit word:
+//  * kNib  (w <= 1, min_ed <= 4): eight 4-bit lanes, band bits 0..2, bit 3 spare
+//  * kByte (w <= 3, min_ed <= 8): four 8-bit lanes, band bits 0..6, bit 7 spare
+// The spare bits of VP, VN and Eq stay 0, so a lane's carry stops in its own
+// spare bit; D0 is masked to the band before it is shifted.  The match masks of
+// all lanes come from one or two PRMTs on a per-row window register W_j whose
+// byte c is the band window of Peq[c] at column j (duplicated into both nibbles
+// for kNib).  Lane counters of the centre bits (weight 2^w per byte) are
+// compared with the threshold by adding 128 - 2^w (L - k) per byte and reading
+// bit 7.
+// ---------------------------------------------------------------------------
+enum LaneMode : int { kModeFull = 0, kModeNib = 1, kModeByte = 2 };
+
+// Column units of the banded modes.  kNib: 8 columns, one 32-bit word per
+// position (bits 0..15: chars of columns 0,2,4,6 as nibbles; bits 16..31:
+// columns 1,3,5,7).  kByte: 4 columns, 16 bits per position (nibble l = char
+// of column l), two positions per word.
+template <int MODE>
+struct BandUnit {
+    static constexpr int kCols = MODE == kModeNib ? 8 : 4;
+    static constexpr int kVec = MODE == kModeNib ? 4 : 2;  // uint4 per unit
+    static constexpr int kBytes = kVec * 16;
+};
+
+// Per-row band windows W_j, j = 0..L-1 (column j+1).
+template <int L, int MODE>
+__device__ __forceinline__ void band_windows(uint32_t word, int w, uint32_t (&W)[L])
+{
+    uint32_t pe[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < L; ++k) {
+        const uint32_t c = (word >> (2 * k)) & 3u;
+        const uint32_t bit = 1u << k;
+        pe[0] |= (c == 0u) ? bit : 0u;
+        pe[1] |= (c == 1u) ? bit : 0u;
+        pe[2] |= (c == 2u) ? bit : 0u;
+        pe[3] |= (c == 3u) ? bit : 0u;
+    }
+    const uint32_t bandmask = (1u << (2 * w + 1)) - 1u;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        const int sh = j - w;  // rows i = j + 1 - w + b  <->  Peq bit i - 1
+        uint32_t x = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            uint32_t v = sh >= 0 ? (pe[c] >> sh) : (pe[c] << (-sh));
+            v &= bandmask;
+            if (MODE == kModeNib)
+                v |= v << 4;
+            x |= v << (8 * c);
+        }
+        W[j] = x;
+    }
+}
+
+struct BandConst {
+    uint32_t vp0, bm, c, k;   // initial VP, band mask, centre mask, threshold constant
+    uint32_t one, h16, h28, h31;  // opaque 1, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
+};
+
+// Eight pair tests (one row, eight columns); hit flags at bits 8m+7 of
+// he (column 2m) and ho (column 2m+1).
+template <int L>
+__device__ __forceinline__ void band_nib(const uint32_t (&W)[L], const uint32_t (&sel)[16], const BandConst &q,
+                                         uint32_t &he, uint32_t &ho)
+{
+    uint32_t vp = q.vp0, vn = 0u, ae = 0u, ao = 0u;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        const uint32_t s = sel[j];
+        const uint32_t e1 = __byte_perm(W[j], W[j], s);
+        const uint32_t e2 = __byte_perm(W[j], W[j], __umulhi(s, q.h16));
+        const uint32_t eq = (e1 & 0x0f0f0f0fu) | (e2 & 0xf0f0f0f0u);
+        const uint32_t x = eq | vn;
+        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t d0 = ((sum ^ vp) | x) & q.bm;
+        const uint32_t hn = vp & d0;
+        const uint32_t hp = vn | ~(d0 | vp);
+        ae = imad(d0 & q.c, q.one, ae);
+        ao = imad(__umulhi(d0, q.h28) & q.c, q.one, ao);
+        const uint32_t ys = __umulhi(d0, q.h31) & q.bm;
+        vn = ys & hp;
+        vp = hn | ~(ys | hp);
+    }
+    he = imad(ae, q.one, q.k) & 0x80808080u;
+    ho = imad(ao, q.one, q.k) & 0x80808080u;
+}
+
+// Four pair tests (one row, four columns); hit flag of column l at bit 8l+7.
+template <int L>
+__device__ __forceinline__ uint32_t band_byte(const uint32_t (&W)[L], const uint32_t (&sel)[8], const BandConst &q)
+{
+    uint32_t vp = q.vp0, vn = 0u, acc = 0u;
+#pragma unroll
+    for (int j = 0; j < L; ++j) {
+        const uint32_t s = (j & 1) ? __umulhi(sel[j >> 1], q.h16) : sel[j >> 1];
+        const uint32_t eq = __byte_perm(W[j], W[j], s);
+        const uint32_t x = eq | vn;
+        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t d0 = ((sum ^ vp) | x) & q.bm;
+        const uint32_t hn = vp & d0;
+        const uint32_t hp = vn | ~(d0 | vp);
+        acc = imad(d0 & q.c, q.one, acc);
+        const uint32_t ys = __umulhi(d0, q.h31) & q.bm;
+        vn = ys & hp;
+        vp = hn | ~(ys | hp);
+    }
+    return imad(acc, q.one, q.k) & 0x80808080u;
+}
+
+// Per-job constants of the banded modes (host and device).
+__host__ __device__ inline int band_mode(int len, int min_ed)
+{
+    (void)len;
+    if (min_ed >= 1 && min_ed <= 4)
+        return kModeNib;
+    if (min_ed >= 5 && min_ed <= 8)
+        return kModeByte;
+    return kModeFull;
+}
+
+__host__ __device__ inline void band_constants(int len, int min_ed, int mode, int &w, uint32_t &vp0, uint32_t &bm,
+                                               uint32_t &c, uint32_t &k)
+{
+    const int kk = min_ed - 1;
+    w = kk / 2;
+    const int B = 2 * w + 1;
+    const uint32_t lane_bm = (1u << B) - 1u;
+    const uint32_t lane_vp = lane_bm & ~((1u << w) - 1u);  // band rows i >= 1: bits w..2w
+    const uint32_t rep = mode == kModeNib ? 0x11111111u : 0x01010101u;
+    bm = lane_bm * rep;
+    vp0 = lane_vp * rep;
+    c = (1u << w) * 0x01010101u;
+    int thr = (1 << w) * (len - kk);
+    if (thr < 0)
+        thr = 0;
+    k = (uint32_t)(128 - thr) * 0x01010101u;
+}
+
 }  // namespace myers
 }  // namespace ig

@@ -142,6 +142,8 @@ def uniform_filtered(count: int, L: int, seed: int, **flt) -> np.ndarray:
 
 def uniform_until(target: int, L: int, seed: int, **flt) -> np.ndarray:
     """Draw uniform strings in seeded batches until `target` survive the filters."""
+    if target <= 0:
+        return np.zeros(0, np.uint32)
     rng = np.random.default_rng(seed)
     out = []
     have = 0
