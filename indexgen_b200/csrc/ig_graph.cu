@@ -225,6 +225,7 @@ struct PairArgs {
     uint32_t hi;
     uint32_t h28;
     uint32_t h31;
+    uint32_t c16;
     unsigned long long *work;
     unsigned long long *rec_count;
     EdgeRecord *rec;
@@ -391,6 +392,8 @@ struct Geo {
     static constexpr int kCols = MODE == kModeFull ? Unit<L>::kCols : BandUnit<MODE>::kCols;
     static constexpr int kVec = MODE == kModeFull ? Unit<L>::kVec : BandUnit<MODE>::kVec;
     static constexpr int kBytes = kVec * 16;
+    static constexpr int kTile = MODE == kModeFull ? kTileCols : BandUnit<MODE>::kTileCols;
+    static_assert(kTile / kCols * kVec <= kTileCols * 2, "a tile must fit one staging slot");
 };
 
 // One (band, segment) item of job J: stream the segment's column tiles through
@@ -423,6 +426,7 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
         q.c = J.cmask;
         q.k = J.kthr;
         q.one = a.one;
+        q.c16 = a.c16;
         q.h16 = a.hi;
         q.h28 = a.h28;
         q.h31 = a.h31;
@@ -434,14 +438,14 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     const long long row_end = (long long)row0 + kBandRows;
     const bool check = ((long long)c_lo < row_end) || (row_end > (long long)J.n) ||
                        (G::kCols > 1 && (c_hi % G::kCols) != 0);
-    const int ntiles = (c_hi - c_lo + kTileCols - 1) / kTileCols;
+    const int ntiles = (c_hi - c_lo + G::kTile - 1) / G::kTile;
     const uint4 *units = a.units + J.unit_off;
     uint32_t rank = 0;
 
     if (tid == 0) {
         for (int t = 0; t < 2 && t < ntiles; ++t) {
-            const int32_t c0 = c_lo + t * kTileCols;
-            const int nu = (min(kTileCols, c_hi - c0) + G::kCols - 1) / G::kCols;
+            const int32_t c0 = c_lo + t * G::kTile;
+            const int nu = (min(G::kTile, c_hi - c0) + G::kCols - 1) / G::kCols;
             const uint32_t bytes = (uint32_t)nu * G::kBytes;
             mbar_arrive_expect_tx(&bar[t], bytes);
             bulk_g2s(&tile[t][0], units + (size_t)(c0 / G::kCols) * G::kVec, bytes, &bar[t]);
@@ -465,8 +469,8 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
             aborted = true;
             return;
         }
-        const int32_t c0 = c_lo + t * kTileCols;
-        const int nu = (min(kTileCols, c_hi - c0) + G::kCols - 1) / G::kCols;
+        const int32_t c0 = c_lo + t * G::kTile;
+        const int nu = (min(G::kTile, c_hi - c0) + G::kCols - 1) / G::kCols;
         if constexpr (MODE == kModeFull) {
             if (check)
                 tile_pass<L, true>(a, tile[b], nu, c0, r, rank, lane);
@@ -480,8 +484,8 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
         }
         __syncthreads();
         if (tid == 0 && t + 2 < ntiles) {
-            const int32_t cn = c_lo + (t + 2) * kTileCols;
-            const int nun = (min(kTileCols, c_hi - cn) + G::kCols - 1) / G::kCols;
+            const int32_t cn = c_lo + (t + 2) * G::kTile;
+            const int nun = (min(G::kTile, c_hi - cn) + G::kCols - 1) / G::kCols;
             const uint32_t bytes = (uint32_t)nun * G::kBytes;
             mbar_arrive_expect_tx(&bar[b], bytes);
             bulk_g2s(&tile[b][0], units + (size_t)(cn / G::kCols) * G::kVec, bytes, &bar[b]);
@@ -512,7 +516,7 @@ __device__ __forceinline__ void dispatch_item(int L, const PairArgs &a, const Jo
     ((L == Ls + 1 ? dispatch_mode<Ls + 1>(J.mode, a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
 }
 
-__global__ void __launch_bounds__(kBandRows) pair_kernel(PairArgs a)
+__global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
 {
     __shared__ __align__(128) uint4 tile[2][kSlotVec];
     __shared__ __align__(8) uint64_t bar[2];
@@ -839,6 +843,7 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.hi = 1u << 16;
     a.h28 = 1u << 28;
     a.h31 = 1u << 31;
+    a.c16 = 16u;
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);

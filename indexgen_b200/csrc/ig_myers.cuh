@@ -167,6 +167,7 @@ struct BandUnit {
     static constexpr int kCols = MODE == kModeNib ? 8 : 4;
     static constexpr int kVec = MODE == kModeNib ? 4 : 2;  // uint4 per unit
     static constexpr int kBytes = kVec * 16;
+    static constexpr int kTileCols = 1024;                  // columns per staged tile (8 KiB)
 };
 
 // Per-row band windows W_j, j = 0..L-1 (column j+1).
@@ -191,18 +192,15 @@ __device__ __forceinline__ void band_windows(uint32_t word, int w, uint32_t (&W)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             uint32_t v = sh >= 0 ? (pe[c] >> sh) : (pe[c] << (-sh));
-            v &= bandmask;
-            if (MODE == kModeNib)
-                v |= v << 4;
-            x |= v << (8 * c);
+            x |= (v & bandmask) << (8 * c);
         }
         W[j] = x;
     }
 }
 
 struct BandConst {
-    uint32_t vp0, bm, c, k;   // initial VP, band mask, centre mask, threshold constant
-    uint32_t one, h16, h28, h31;  // opaque 1, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
+    uint32_t vp0, bm, c, k;       // initial VP, band mask, centre mask, threshold constant
+    uint32_t one, c16, h16, h28, h31;  // opaque 1, 16, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
 };
 
 // Eight pair tests (one row, eight columns); hit flags at bits 8m+7 of
@@ -211,26 +209,30 @@ template <int L>
 __device__ __forceinline__ void band_nib(const uint32_t (&W)[L], const uint32_t (&sel)[16], const BandConst &q,
                                          uint32_t &he, uint32_t &ho)
 {
-    uint32_t vp = q.vp0, vn = 0u, ae = 0u, ao = 0u;
+    uint32_t vp = q.vp0, vn = 0u, acc = 0u, be = 0u, bo = 0u;
 #pragma unroll
     for (int j = 0; j < L; ++j) {
         const uint32_t s = sel[j];
         const uint32_t e1 = __byte_perm(W[j], W[j], s);
-        const uint32_t e2 = __byte_perm(W[j], W[j], __umulhi(s, q.h16));
-        const uint32_t eq = (e1 & 0x0f0f0f0fu) | (e2 & 0xf0f0f0f0u);
-        const uint32_t x = eq | vn;
-        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t whi = imad(W[j], q.c16, 0u);
+        const uint32_t e2 = __byte_perm(whi, whi, __umulhi(s, q.h16));
+        const uint32_t x = e1 | e2 | vn;
+        const uint32_t sum = imad((e1 | e2) & vp, q.one, vp);
         const uint32_t d0 = ((sum ^ vp) | x) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
-        ae = imad(d0 & q.c, q.one, ae);
-        ao = imad(__umulhi(d0, q.h28) & q.c, q.one, ao);
+        acc = imad(d0 & q.c, q.one, acc);
+        if ((j + 1) % 7 == 0 || j == L - 1) {
+            be = imad(acc & 0x0f0f0f0fu, q.one, be);
+            bo = imad(__umulhi(acc, q.h28) & 0x0f0f0f0fu, q.one, bo);
+            acc = 0u;
+        }
         const uint32_t ys = __umulhi(d0, q.h31) & q.bm;
         vn = ys & hp;
         vp = hn | ~(ys | hp);
     }
-    he = imad(ae, q.one, q.k) & 0x80808080u;
-    ho = imad(ao, q.one, q.k) & 0x80808080u;
+    he = imad(be, q.one, q.k) & 0x80808080u;
+    ho = imad(bo, q.one, q.k) & 0x80808080u;
 }
 
 // Four pair tests (one row, four columns); hit flag of column l at bit 8l+7.
@@ -277,7 +279,7 @@ __host__ __device__ inline void band_constants(int len, int min_ed, int mode, in
     const uint32_t rep = mode == kModeNib ? 0x11111111u : 0x01010101u;
     bm = lane_bm * rep;
     vp0 = lane_vp * rep;
-    c = (1u << w) * 0x01010101u;
+    c = (1u << w) * rep;
     int thr = (1 << w) * (len - kk);
     if (thr < 0)
         thr = 0;
