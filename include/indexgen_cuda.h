@@ -158,6 +158,10 @@ typedef struct ig_server_opts {
     int reserved;
     int64_t max_batch_pairs;   /* pair tests per launch (0 = 2e10, ~0.1 s)        */
     int64_t hbm_budget_bytes;  /* estimated HBM per launch (0 = half the free HBM) */
+    int64_t pool_reserve_bytes; /* device memory taken into the context's stream-
+                                 * ordered pool at start, so that the first large
+                                 * jobs do not wait on the driver to map memory
+                                 * (0 = min(4 GiB, budget / 4); < 0 = none)      */
 } ig_server_opts;
 /* Job states reported by ig_server_poll. */
 #define IG_JOB_QUEUED 0

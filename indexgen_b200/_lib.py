@@ -44,7 +44,7 @@ class ServerOpts(ctypes.Structure):
 
     _fields_ = [("host_threads", ctypes.c_int), ("max_batch_jobs", ctypes.c_int), ("order_threads", ctypes.c_int),
                 ("reserved", ctypes.c_int), ("max_batch_pairs", ctypes.c_int64),
-                ("hbm_budget_bytes", ctypes.c_int64)]
+                ("hbm_budget_bytes", ctypes.c_int64), ("pool_reserve_bytes", ctypes.c_int64)]
 
 
 _vp = ctypes.c_void_p

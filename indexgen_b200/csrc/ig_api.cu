@@ -173,9 +173,22 @@ ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *
 
 }  // namespace
 
+bool reserve_pool(Ctx *ctx, size_t bytes)
+{
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaFreeAsync(p, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(ctx->stream);
+    cudaGetLastError();
+    return e == cudaSuccess;
+}
+
 // What the host greedy needs of a graph, downloaded once: the canonical
 // adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
-
 ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
 {
     ig_graph *g = static_cast<ig_graph *>(gg);

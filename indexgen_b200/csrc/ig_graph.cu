@@ -702,13 +702,22 @@ ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
 {
     if (b.bytes >= bytes && b.ptr)
         return IG_OK;
+    // A buffer that has to grow again grows by at least half: every growth
+    // of a workspace costs a stream-ordered free + allocation, and growth of
+    // the edge records also a second pair pass.
+    size_t want = std::max<size_t>(bytes, 256);
     if (b.ptr) {
+        want = std::max(want, b.bytes + b.bytes / 2);
         cudaFreeAsync(b.ptr, ctx->stream);
         b.ptr = nullptr;
         b.bytes = 0;
     }
-    size_t want = std::max<size_t>(bytes, 256);
     cudaError_t e = cudaMallocAsync(&b.ptr, want, ctx->stream);
+    if (e != cudaSuccess && want > bytes) {  // the headroom does not fit: the exact size may
+        cudaGetLastError();
+        want = std::max<size_t>(bytes, 256);
+        e = cudaMallocAsync(&b.ptr, want, ctx->stream);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         b.ptr = nullptr;

@@ -112,6 +112,10 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
 // In-place inclusive scan of m int64 on the context stream (ig_graph.cu).
 ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m);
 ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what);
+// Takes `bytes` into the device's stream-ordered pool (allocated and freed
+// once; the pool keeps freed memory) so that later workspace and output
+// allocations are served from it instead of new driver mappings (ig_api.cu).
+bool reserve_pool(Ctx *ctx, size_t bytes);
 // Symmetric CSR in the canonical neighbour order (ig_adjacency.cu).
 ig_status build_adjacency(Ctx *ctx, Graph *g);
 

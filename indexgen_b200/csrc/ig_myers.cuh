@@ -148,13 +148,18 @@ __device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint
 // Many pair tests share one 32-bit word:
 //  * kNib  (w <= 1, min_ed <= 4): eight 4-bit lanes, band bits 0..2, bit 3 spare
 //  * kByte (w <= 3, min_ed <= 8): four 8-bit lanes, band bits 0..6, bit 7 spare
-// The spare bits of VP, VN and Eq stay 0, so a lane's carry stops in its own
-// spare bit; D0 is masked to the band before it is shifted.  The match masks of
-// all lanes come from one or two PRMTs on a per-row window register W_j whose
-// byte c is the band window of Peq[c] at column j (duplicated into both nibbles
-// for kNib).  Lane counters of the centre bits (weight 2^w per byte) are
-// compared with the threshold by adding 128 - 2^w (L - k) per byte and reading
-// bit 7.
+// The spare bits of VP and Eq stay 0, so a lane's carry stops in its own spare
+// bit; D0 is masked to the band before it is shifted.  Y is not masked: its
+// spare bit may hold the next lane's bit 0, which reaches VN's spare bit only
+// (HP's spare bit is always 1, so VP's stays 0) and is masked out of D0.
+// Per character step kNib issues 10 ALU-pipe ops (2 PRMT + 8 LOP3) and 6
+// FMA-pipe ops (IMAD / IMAD.HI) for eight pair tests, kByte 9 ALU + 3.5 FMA
+// for four.  The match masks of all lanes come from PRMTs on a per-row window
+// register W_j whose byte c is the band window of Peq[c] at column j (kNib:
+// one PRMT on W_j for the even lanes' low nibbles, one on W_j * 16 for the
+// odd lanes' high nibbles).  Lane counters of the centre bits (weight 2^w
+// per byte) are compared with the threshold by adding 128 - 2^w (L - k) per
+// byte and reading bit 7.
 // ---------------------------------------------------------------------------
 enum LaneMode : int { kModeFull = 0, kModeNib = 1, kModeByte = 2 };
 
@@ -216,9 +221,11 @@ __device__ __forceinline__ void band_nib(const uint32_t (&W)[L], const uint32_t 
         const uint32_t e1 = __byte_perm(W[j], W[j], s);
         const uint32_t whi = imad(W[j], q.c16, 0u);
         const uint32_t e2 = __byte_perm(whi, whi, __umulhi(s, q.h16));
-        const uint32_t x = e1 | e2 | vn;
-        const uint32_t sum = imad((e1 | e2) & vp, q.one, vp);
-        const uint32_t d0 = ((sum ^ vp) | x) & q.bm;
+        // e1 holds low nibbles only and e2 high nibbles only, so e1 | e2 is a
+        // sum, which the FMA pipe can form
+        const uint32_t eq = imad(e1, q.one, e2);
+        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t d0 = ((sum ^ vp) | eq | vn) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
         acc = imad(d0 & q.c, q.one, acc);
@@ -227,7 +234,7 @@ __device__ __forceinline__ void band_nib(const uint32_t (&W)[L], const uint32_t 
             bo = imad(__umulhi(acc, q.h28) & 0x0f0f0f0fu, q.one, bo);
             acc = 0u;
         }
-        const uint32_t ys = __umulhi(d0, q.h31) & q.bm;
+        const uint32_t ys = __umulhi(d0, q.h31);  // spare bits may pick up a neighbour's bit 0
         vn = ys & hp;
         vp = hn | ~(ys | hp);
     }
@@ -244,13 +251,12 @@ __device__ __forceinline__ uint32_t band_byte(const uint32_t (&W)[L], const uint
     for (int j = 0; j < L; ++j) {
         const uint32_t s = (j & 1) ? __umulhi(sel[j >> 1], q.h16) : sel[j >> 1];
         const uint32_t eq = __byte_perm(W[j], W[j], s);
-        const uint32_t x = eq | vn;
         const uint32_t sum = imad(eq & vp, q.one, vp);
-        const uint32_t d0 = ((sum ^ vp) | x) & q.bm;
+        const uint32_t d0 = ((sum ^ vp) | eq | vn) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
         acc = imad(d0 & q.c, q.one, acc);
-        const uint32_t ys = __umulhi(d0, q.h31) & q.bm;
+        const uint32_t ys = __umulhi(d0, q.h31);
         vn = ys & hp;
         vp = hn | ~(ys | hp);
     }

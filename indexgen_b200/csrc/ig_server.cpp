@@ -236,6 +236,10 @@ ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **
             cudaSetDevice(prev);
         o.hbm_budget_bytes = (int64_t)(free_b / 2);
     }
+    if (o.pool_reserve_bytes == 0)
+        o.pool_reserve_bytes = std::min<int64_t>((int64_t)4 << 30, o.hbm_budget_bytes / 4);
+    if (o.pool_reserve_bytes > 0)
+        ig::reserve_pool(ctx, (size_t)o.pool_reserve_bytes);  // best effort
     sv->opts = o;
     sv->scheduler = std::thread([sv] { sv->schedule_loop(); });
     for (int i = 0; i < o.host_threads; ++i)

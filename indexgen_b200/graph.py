@@ -289,9 +289,11 @@ class Server:
     STATES = ("queued", "on_device", "greedy", "done", "cancelled", "failed")
 
     def __init__(self, ctx: Context | None = None, host_threads: int = 0, max_batch_jobs: int = 0,
-                 max_batch_pairs: int = 0, hbm_budget_bytes: int = 0, order_threads: int = 1):
+                 max_batch_pairs: int = 0, hbm_budget_bytes: int = 0, order_threads: int = 1,
+                 pool_reserve_bytes: int = 0):
         self.ctx = ctx or default_context()
-        o = _lib.ServerOpts(host_threads, max_batch_jobs, order_threads, 0, max_batch_pairs, hbm_budget_bytes)
+        o = _lib.ServerOpts(host_threads, max_batch_jobs, order_threads, 0, max_batch_pairs, hbm_budget_bytes,
+                            pool_reserve_bytes)
         h = ctypes.c_void_p()
         check(lib().ig_server_create(self.ctx.handle, ctypes.byref(o), ctypes.byref(h)), "ig_server_create",
               self.ctx.handle)
