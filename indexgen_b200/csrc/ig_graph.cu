@@ -9,15 +9,15 @@
 //   prep_units      words -> PRMT selector streams, two columns per unit for L <= 15
 //   pair_kernel     ONE persistent launch for the whole batch: CTAs take
 //                   (job, row band, column segment) items from an atomic queue and
-//                   dispatch on the job's L; 256 rows per band live in registers as two PRMT
-//                   pools of Myers Peq masks; column tiles of the segment are
-//                   staged into shared memory by cp.async.bulk (TMA bulk copy, no
-//                   multicast) with a two-slot mbarrier pipeline; each thread runs
-//                   the 32-bit Myers recurrence on two columns at once (two
-//                   16-bit lanes, L <= 15) or one (L = 16) and emits hits
-//                   through warp ballot + one atomic per warp as
-//                   (row, col, rank-in-(row,segment), cell) records, plus a
-//                   per-(row, segment) count.
+//                   dispatch on the job's L and lane form; 256 rows per band, one
+//                   per thread, keep their match masks in registers; column tiles
+//                   of the segment are staged into shared memory by cp.async.bulk
+//                   (TMA bulk copy, no multicast) with a two-slot mbarrier
+//                   pipeline; each thread tests its row against 8 (banded nibble
+//                   lanes, editDist <= 4), 4 (byte lanes, editDist <= 8) or 2/1
+//                   (full Myers) columns per 32-bit word and emits hits as
+//                   (row, col, rank-in-(row,segment), cell) records into slots
+//                   its warp takes in chunks, plus a per-(row, segment) count.
 //   row_prefix      per-row exclusive prefix over its segments + degree
 //   scan            exclusive scan of degrees -> row_ptr (int64)
 //   scatter         cols[row_ptr[r] + prefix[cell] + rank] = col
@@ -227,7 +227,8 @@ struct PairArgs {
     uint32_t h31;
     uint32_t c16;
     unsigned long long *work;
-    unsigned long long *rec_count;
+    unsigned long long *rec_count;  // record slots handed out (chunks of kSlotChunk)
+    unsigned long long *hit_count;  // pair tests that are edges (exact)
     EdgeRecord *rec;
     unsigned long long rec_cap;
     uint32_t *counts;
@@ -235,29 +236,52 @@ struct PairArgs {
     int emit;
 };
 
-__device__ __forceinline__ void emit_hit(const PairArgs &a, bool hit, uint32_t row, uint32_t col, uint32_t cell,
-                                         uint32_t &rank, int lane)
+// Record slots.  Each warp takes slots from the global counter in chunks of
+// kSlotChunk (one atomic per chunk instead of one per hit group: a single
+// counter address is otherwise the limit on dense graphs) and keeps the rest
+// of its chunk in shared memory.  Slots a warp never fills are written as
+// sentinels (row = kNoRow) when the kernel ends; the scatter skips them.
+constexpr unsigned kSlotChunk = 64;
+constexpr uint32_t kNoRow = 0xffffffffu;
+
+// Two scalar arrays, each element read and written on its own (a 16-byte
+// struct here, read whole, faulted with a misaligned shared access).
+__shared__ unsigned long long g_slot_base[kBandRows / 32];  // next free slot of each warp's chunk
+__shared__ unsigned g_slot_left[kBandRows / 32];            // free slots left in it
+
+// Slots of the warp's next `total` records (warp-uniform call): record j goes
+// to b0 + j for j < n0, else to b1 + (j - n0).
+struct Slots {
+    unsigned long long b0, b1;
+    unsigned n0;
+};
+
+__device__ __forceinline__ Slots take_slots(const PairArgs &a, unsigned total, int lane)
 {
-    const unsigned m = __ballot_sync(kFull, hit);
-    if (m == 0u)
-        return;
-    const int leader = __ffs(m) - 1;
-    unsigned long long base = 0;
-    if (lane == leader)
-        base = atomicAdd(a.rec_count, (unsigned long long)__popc(m));
-    base = __shfl_sync(kFull, base, leader);
-    if (hit) {
-        const unsigned long long idx = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
-        if (a.emit && idx < a.rec_cap) {
-            EdgeRecord r;
-            r.row = row;
-            r.col = col;
-            r.rank = rank;
-            r.cell = cell;
-            *reinterpret_cast<uint4 *>(a.rec + idx) = *reinterpret_cast<const uint4 *>(&r);
+    const int w = threadIdx.x >> 5;
+    unsigned long long b0 = 0, b1 = 0;
+    unsigned n0 = 0;
+    if (lane == 0) {
+        b0 = g_slot_base[w];
+        const unsigned left = g_slot_left[w];
+        if (left >= total) {
+            n0 = total;
+            g_slot_base[w] = b0 + total;
+            g_slot_left[w] = left - total;
+        } else {
+            n0 = left;
+            const unsigned need = total - left;
+            const unsigned take = need > kSlotChunk ? need : kSlotChunk;
+            b1 = atomicAdd(a.rec_count, (unsigned long long)take);
+            g_slot_base[w] = b1 + need;
+            g_slot_left[w] = take - need;
         }
-        ++rank;
     }
+    Slots s;
+    s.b0 = __shfl_sync(kFull, b0, 0);
+    s.b1 = __shfl_sync(kFull, b1, 0);
+    s.n0 = __shfl_sync(kFull, n0, 0);
+    return s;
 }
 
 // Everything one thread needs about its row while it walks a segment.
@@ -271,6 +295,56 @@ struct RowCtx {
     int32_t n;
     int lim;
 };
+
+// Bits [lo, hi) of the columns col0 + c, c < NC, that lie in the strict upper
+// triangle of the job (col > row, col < n) for a valid row.
+template <int NC>
+__device__ __forceinline__ uint32_t upper_mask(const RowCtx &r, int32_t col0)
+{
+    if (!r.ok)
+        return 0u;
+    const int lo = max(r.row + 1 - col0, 0);
+    const int hi = min(r.n - col0, NC);
+    return hi > lo ? (((1u << hi) - 1u) & ~((1u << lo) - 1u)) : 0u;
+}
+
+// Emit this thread's hits m (bit c: column col0 + c, c < NC) for a warp in
+// which at least one lane has a hit.  Ranks count the row's hits in its
+// (row, segment) cell in column order, so the scatter needs no sort.
+template <int NC>
+__device__ __forceinline__ void emit_mask(const PairArgs &a, uint32_t m, const RowCtx &r, int32_t col0,
+                                          uint32_t &rank, int lane)
+{
+    const uint32_t cnt = __popc(m);
+    if (!a.emit) {
+        rank += cnt;
+        return;
+    }
+    // warp total and this lane's exclusive prefix from the bit planes of cnt
+    constexpr int kPlanes = NC >= 8 ? 4 : (NC >= 4 ? 3 : (NC >= 2 ? 2 : 1));
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned total = 0, pre = 0;
+#pragma unroll
+    for (int b = 0; b < kPlanes; ++b) {
+        const unsigned bal = __ballot_sync(kFull, (cnt >> b) & 1u);
+        total += (unsigned)__popc(bal) << b;
+        pre += (unsigned)__popc(bal & lt) << b;
+    }
+    if (total == 0u)
+        return;
+    const Slots sl = take_slots(a, total, lane);
+    unsigned j = pre;
+    while (m) {
+        const int c = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned long long idx = j < sl.n0 ? sl.b0 + j : sl.b1 + (j - sl.n0);
+        if (idx < a.rec_cap) {
+            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(r.grow, r.base + (uint32_t)(col0 + c), rank, r.cell);
+        }
+        ++rank;
+        ++j;
+    }
+}
 
 // One staged tile of nu units whose first (job-local) column is c0.  CHECK
 // adds the strict-upper-triangle test (col > row), row < n and col < n; it is
@@ -299,14 +373,11 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
             bool h0, h1;
             myers_two<L>(r.p01, r.p23, sel, a.one, a.two, r.lim, h0, h1);
             const int32_t col = c0 + 2 * u;
-            if (CHECK) {
-                h0 = h0 && r.ok && (col > r.row) && (col < r.n);
-                h1 = h1 && r.ok && (col + 1 > r.row) && (col + 1 < r.n);
-            }
-            if (__any_sync(kFull, h0 || h1)) {
-                emit_hit(a, h0, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
-                emit_hit(a, h1, r.grow, r.base + (uint32_t)(col + 1), r.cell, rank, lane);
-            }
+            uint32_t m = (h0 ? 1u : 0u) | (h1 ? 2u : 0u);
+            if (CHECK)
+                m &= upper_mask<2>(r, col);
+            if (__any_sync(kFull, m != 0u))
+                emit_mask<2>(a, m, r, col, rank, lane);
         } else {
             static_assert(U::kUsed == 2, "one-lane units are two uint4");
             uint32_t sel[8];
@@ -314,12 +385,13 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
             const uint4 q1 = src[1];
             sel[0] = q0.x; sel[1] = q0.y; sel[2] = q0.z; sel[3] = q0.w;
             sel[4] = q1.x; sel[5] = q1.y; sel[6] = q1.z; sel[7] = q1.w;
-            bool h0 = myers_one<L>(r.p01, r.p23, sel, a.one, a.two, a.hi, r.lim);
+            const bool h0 = myers_one<L>(r.p01, r.p23, sel, a.one, a.two, a.hi, r.lim);
             const int32_t col = c0 + u;
+            uint32_t m = h0 ? 1u : 0u;
             if (CHECK)
-                h0 = h0 && r.ok && (col > r.row);
-            if (__any_sync(kFull, h0))
-                emit_hit(a, h0, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
+                m &= upper_mask<1>(r, col);
+            if (__any_sync(kFull, m != 0u))
+                emit_mask<1>(a, m, r, col, rank, lane);
         }
     }
 }
@@ -368,18 +440,19 @@ __device__ __forceinline__ void tile_pass_band(const PairArgs &a, const uint4 *t
         }
         if (__any_sync(kFull, (he | ho) != 0u)) {
             const int32_t base_col = c0 + u * BU::kCols;
+            // hit flags sit at bits 8q+7: he of column 2q (kNib) or q (kByte), ho of column 2q+1
+            uint32_t m = 0u;
 #pragma unroll
-            for (int c = 0; c < BU::kCols; ++c) {
-                bool hit;
+            for (int q = 0; q < 4; ++q) {
                 if (MODE == kModeNib)
-                    hit = (((c & 1) ? ho : he) >> (8 * (c >> 1) + 7)) & 1u;
+                    m |= (((he >> (8 * q + 7)) & 1u) << (2 * q)) | (((ho >> (8 * q + 7)) & 1u) << (2 * q + 1));
                 else
-                    hit = (he >> (8 * c + 7)) & 1u;
-                const int32_t col = base_col + c;
-                if (CHECK)
-                    hit = hit && r.ok && (col > r.row) && (col < r.n);
-                emit_hit(a, hit, r.grow, r.base + (uint32_t)col, r.cell, rank, lane);
+                    m |= ((he >> (8 * q + 7)) & 1u) << q;
             }
+            if (CHECK)
+                m &= upper_mask<BU::kCols>(r, base_col);
+            if (__any_sync(kFull, m != 0u))
+                emit_mask<BU::kCols>(a, m, r, base_col, rank, lane);
         }
     }
 }
@@ -493,6 +566,9 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     }
     if (r.ok)
         a.counts[r.cell] = rank;
+    const unsigned hits = __reduce_add_sync(kFull, r.ok ? rank : 0u);
+    if (lane == 0 && hits != 0u)
+        atomicAdd(a.hit_count, (unsigned long long)hits);
 }
 
 template <int L>
@@ -527,6 +603,10 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
         mbar_init(&bar[0], 1);
         mbar_init(&bar[1], 1);
         mbar_fence_init();
+    }
+    if ((tid & 31) == 0) {
+        g_slot_base[tid >> 5] = 0ull;
+        g_slot_left[tid >> 5] = 0u;
     }
     __syncthreads();
     uint32_t parity = 0u;  // bit b: phase parity of slot b
@@ -565,6 +645,16 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
         if (aborted)
             break;
         __syncthreads();
+    }
+    // the unused rest of each warp's slot chunk becomes sentinels
+    if (a.emit && !aborted) {
+        const unsigned long long base = g_slot_base[tid >> 5];
+        const unsigned left = g_slot_left[tid >> 5];
+        for (unsigned k = tid & 31; k < left; k += 32) {
+            const unsigned long long idx = base + k;
+            if (idx < a.rec_cap)
+                *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(kNoRow, 0u, 0u, 0u);
+        }
     }
 }
 
@@ -693,6 +783,8 @@ __global__ void scatter_records(const EdgeRecord *__restrict__ rec, unsigned lon
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < nrec;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const uint4 r = *reinterpret_cast<const uint4 *>(rec + i);
+        if (r.x == kNoRow)
+            continue;
         const int64_t pos = row_ptr[r.x] + (int64_t)counts[r.w] + (int64_t)r.z;
         cols[pos] = (int32_t)r.y;
     }
@@ -815,8 +907,10 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
 
 // Runs prep + the pair kernel for a planned batch.  On return *total holds
 // the number of edges; records are complete iff *total <= capacity.
+// One pair pass.  *slots = record slots handed out (>= *hits; the records
+// buffer must hold them all for the pass to be complete), *hits = edges.
 ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int grid, int emit,
-                    unsigned long long *total)
+                    unsigned long long *slots, unsigned long long *hits)
 {
     cudaStream_t st = ctx->stream;
     ig_status s;
@@ -856,6 +950,7 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);
+    a.hit_count = flags + 3;
     a.rec = static_cast<EdgeRecord *>(ctx->records.ptr);
     a.rec_cap = emit ? ctx->rec_capacity : 0;
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
@@ -871,7 +966,8 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     phase_collect(ctx);
     if (static_cast<int>(host_flags[2] & 0xffffffffu) == kStatusTimeout)
         return set_error(ctx, IG_ERR_TIMEOUT, "pair kernel: staged tile never arrived (bounded wait expired)");
-    *total = host_flags[1];
+    *slots = host_flags[1];
+    *hits = host_flags[3];
     return IG_OK;
 }
 
@@ -989,11 +1085,11 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         *edges = 0;
         return IG_OK;
     }
-    unsigned long long total = 0;
-    s = run_pairs(ctx, d_words, B, grid, 0, &total);
+    unsigned long long slots = 0, hits = 0;
+    s = run_pairs(ctx, d_words, B, grid, 0, &slots, &hits);
     if (s != IG_OK)
         return s;
-    *edges = (int64_t)total;
+    *edges = (int64_t)hits;
     return IG_OK;
 }
 
@@ -1025,16 +1121,19 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
             return s;
         ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
     }
-    unsigned long long total = 0;
+    unsigned long long slots = 0, total = 0;
     for (int attempt = 0;; ++attempt) {
-        s = run_pairs(ctx, d_words, B, grid, 1, &total);
+        s = run_pairs(ctx, d_words, B, grid, 1, &slots, &total);
         if (s != IG_OK)
             return s;
-        if (total <= ctx->rec_capacity)
+        if (slots <= ctx->rec_capacity)
             break;
         if (attempt > 0)
-            return set_error(ctx, IG_ERR_STATE, "edge count changed between identical passes");
-        const size_t want = (size_t)(total + total / 8 + 1024);
+            return set_error(ctx, IG_ERR_STATE, "record slots exceeded a buffer sized for them twice");
+        // slots of a rerun differ from this pass only by the chunk tails of
+        // the warps (scheduling), so leave room for all of them
+        const size_t tails = (size_t)grid * (kBandRows / 32) * kSlotChunk;
+        const size_t want = (size_t)(total + total / 8) + tails + 1024;
         s = ensure(ctx, ctx->records, want * sizeof(EdgeRecord), "edge records");
         if (s != IG_OK)
             return s;
@@ -1056,8 +1155,8 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         return s;
     if (total > 0) {
         const int sgrid =
-            (int)std::min<unsigned long long>((total + 255) / 256, (unsigned long long)ctx->sm_count * 16);
-        scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), total,
+            (int)std::min<unsigned long long>((slots + 255) / 256, (unsigned long long)ctx->sm_count * 16);
+        scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), slots,
                                                 g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
                                                 g->d_cols);
         ctx->launches++;
