@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <memory>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -124,8 +125,9 @@ ig_status fetch_host(ig_graph *g)
     return IG_OK;
 }
 
-// Canonical symmetric adjacency on the device (built once), then on the host.
-ig_status fetch_adjacency(ig_graph *g, std::vector<int64_t> &ap, std::vector<int32_t> &adj)
+// Canonical symmetric adjacency on the device (built once), then into one
+// host block (pinned when the pool has room): offsets first, then neighbours.
+ig_status fetch_adjacency(ig_graph *g, HostGraph &hg)
 {
     ig::Ctx *ctx = g->ctx;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -133,21 +135,28 @@ ig_status fetch_adjacency(ig_graph *g, std::vector<int64_t> &ap, std::vector<int
     ig_status s = build_adjacency(ctx, g);
     if (s != IG_OK)
         return s;
-    try {
-        ap.resize((size_t)g->n + 1);
-        adj.resize((size_t)std::max<int64_t>(2 * g->edges, 1));
-    } catch (...) {
-        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
+    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
+    const size_t adj_bytes = (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
+    std::shared_ptr<void> block = ctx->pinned->acquire(ptr_bytes + adj_bytes);
+    if (!block) {
+        void *p = std::malloc(ptr_bytes + adj_bytes);  // uninitialised: the copy fills it
+        if (!p)
+            return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
+        block = std::shared_ptr<void>(p, std::free);
     }
-    cudaError_t e = cudaMemcpyAsync(ap.data(), g->d_adj_ptr, ((size_t)g->n + 1) * sizeof(int64_t),
-                                    cudaMemcpyDeviceToHost, ctx->stream);
+    int64_t *ap = static_cast<int64_t *>(block.get());
+    int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
+    cudaError_t e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess && g->edges > 0)
-        e = cudaMemcpyAsync(adj.data(), g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+        e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             ctx->stream);
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess)
         return cuda_error(ctx, e, "adjacency download");
+    hg.ptr = ap;
+    hg.idx = adj;
+    hg.storage = std::move(block);
     return IG_OK;
 }
 
@@ -187,6 +196,45 @@ bool reserve_pool(Ctx *ctx, size_t bytes)
     return e == cudaSuccess;
 }
 
+std::shared_ptr<void> PinnedPool::acquire(size_t bytes)
+{
+    size_t cls = (size_t)1 << 20;
+    while (cls < bytes)
+        cls <<= 1;
+    void *p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = free_.lower_bound(cls);
+        if (it != free_.end() && it->first <= 4 * cls) {
+            cls = it->first;
+            p = it->second;
+            free_.erase(it);
+        } else {
+            if (total_ + cls > kCap)
+                return nullptr;
+            total_ += cls;  // reserved before the (slow) pinning, outside the lock
+        }
+    }
+    if (!p && cudaHostAlloc(&p, cls, cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(mu_);
+        total_ -= cls;
+        return nullptr;
+    }
+    std::shared_ptr<PinnedPool> self = shared_from_this();
+    return std::shared_ptr<void>(p, [self, cls](void *q) {
+        std::lock_guard<std::mutex> lk(self->mu_);
+        self->free_.emplace(cls, q);
+    });
+}
+
+PinnedPool::~PinnedPool()
+{
+    for (auto &b : free_)
+        cudaFreeHost(b.second);
+    cudaGetLastError();
+}
+
 // What the host greedy needs of a graph, downloaded once: the canonical
 // adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
 ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
@@ -196,13 +244,19 @@ ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
     hg.jobs = g->jobs;
     hg.job_edge_off = g->job_edge_off;
     if (order_threads == 1)
-        return fetch_adjacency(g, hg.ptr, hg.idx);
+        return fetch_adjacency(g, hg);
     ig_status s = fetch_host(g);
-    if (s == IG_OK) {
-        hg.ptr = g->h_row_ptr;
-        hg.idx = g->h_cols;
+    if (s != IG_OK)
+        return s;
+    try {
+        auto csr = std::make_shared<std::pair<std::vector<int64_t>, std::vector<int32_t>>>(g->h_row_ptr, g->h_cols);
+        hg.ptr = csr->first.data();
+        hg.idx = csr->second.data();
+        hg.storage = std::move(csr);
+    } catch (...) {
+        return set_error(g->ctx, IG_ERR_OOM, "host CSR copy failed");
     }
-    return s;
+    return IG_OK;
 }
 
 // Greedy of every job on `host_threads` host threads (pure host work),
@@ -212,8 +266,8 @@ int32_t greedy_one(const HostGraph &hg, int job, int32_t *out)
 {
     const JobSpec &J = hg.jobs[(size_t)job];
     if (hg.order_threads == 1)
-        return greedy_from_adjacency(hg.ptr.data() + J.word_off, hg.idx.data(), J.n, J.word_off, out);
-    return greedy_from_upper(hg.ptr.data() + J.word_off, hg.idx.data(), J.n, J.word_off, hg.order_threads, out);
+        return greedy_from_adjacency(hg.ptr + J.word_off, hg.idx, J.n, J.word_off, out);
+    return greedy_from_upper(hg.ptr + J.word_off, hg.idx, J.n, J.word_off, hg.order_threads, out);
 }
 
 bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts)

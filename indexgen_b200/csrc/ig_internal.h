@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstdint>
+#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -51,6 +53,25 @@ struct DevBuf {
     size_t bytes = 0;
 };
 
+// Page-locked host blocks for graph downloads, recycled across calls: a
+// pageable download of a few hundred MB runs at a few GB/s and first touches
+// fresh pages, a pinned one at tens of GB/s.  Blocks come in power-of-two
+// sizes; the pool holds at most kCap bytes and callers fall back to pageable
+// memory beyond that (ig_api.cu).
+class PinnedPool : public std::enable_shared_from_this<PinnedPool> {
+public:
+    static constexpr size_t kCap = (size_t)16 << 30;
+    // A block of at least `bytes`, returned to the pool when the last copy of
+    // the pointer goes; nullptr when the pool is full or pinning fails.
+    std::shared_ptr<void> acquire(size_t bytes);
+    ~PinnedPool();
+
+private:
+    std::mutex mu_;
+    std::multimap<size_t, void *> free_;
+    size_t total_ = 0;
+};
+
 struct Ctx {
     int device = 0;
     int sm_count = 0;
@@ -68,6 +89,7 @@ struct Ctx {
     double phase_ms[3] = {0, 0, 0};
     int64_t phase_launches[3] = {0, 0, 0};
     bool phase_pending[3] = {false, false, false};
+    std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
 };
 
 // Records an event pair around a phase when profiling is on.
@@ -131,8 +153,9 @@ int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_
 // adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
 struct HostGraph {
     int order_threads = 1;
-    std::vector<int64_t> ptr;  // adjacency or row offsets, [n+1]
-    std::vector<int32_t> idx;  // neighbour / column ids (global)
+    const int64_t *ptr = nullptr;   // adjacency or row offsets, [n+1]
+    const int32_t *idx = nullptr;   // neighbour / column ids (global)
+    std::shared_ptr<void> storage;  // owns ptr and idx (pinned block or heap)
     std::vector<JobSpec> jobs;
     std::vector<int64_t> job_edge_off;
 };

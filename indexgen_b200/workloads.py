@@ -159,13 +159,19 @@ def vt16_words(target: int, seed: int, max_run: int = 3, min_gc: float = 0.3, ma
     """`target` filtered words of sum(i*x_i)=0 mod 17, sum(x_i)=0 mod 4 (n=16)."""
     L = 16
     rng = np.random.default_rng(seed)
+    # per byte b of a word (digits 4b..4b+3): sum of (i+1)*x_i and of x_i
+    byte = np.arange(256, dtype=np.int64)
+    dig = (byte[:, None] >> (2 * np.arange(4))) & 3
+    wsum = [(dig * (4 * b + 1 + np.arange(4))).sum(axis=1) for b in range(4)]
+    dsum = dig.sum(axis=1)
     out = []
     have = 0
-    pos = np.arange(1, L + 1, dtype=np.int64)
     while have < target:
-        d = rng.integers(0, 4, size=(1 << 22, L))
-        ok = ((d * pos).sum(axis=1) % 17 == 0) & (d.sum(axis=1) % 4 == 0)
-        w = pack_digits(d[ok])
+        w = rng.integers(0, 1 << 32, size=1 << 22, dtype=np.uint64).astype(np.uint32)  # 16 uniform digits each
+        bs = [(w >> np.uint32(8 * b)) & np.uint32(0xff) for b in range(4)]
+        ws = wsum[0][bs[0]] + wsum[1][bs[1]] + wsum[2][bs[2]] + wsum[3][bs[3]]
+        ds = dsum[bs[0]] + dsum[bs[1]] + dsum[bs[2]] + dsum[bs[3]]
+        w = w[(ws % 17 == 0) & (ds % 4 == 0)]
         w = w[filter_words(w, L, max_run, min_gc, max_gc)]
         out.append(w)
         have += len(w)

@@ -215,6 +215,95 @@ static int conflict_upper_impl(const uint32_t *words, int32_t n, int len, int mi
     return fail ? -1 : 0;
 }
 
+/* ---------------- full neighbour rows of sampled vertices ---------------- */
+/* For spot checks of graphs too large for the all-pairs oracle: for each
+ * sampled row r, every c != r with ED(w_r, w_c) < min_ed, ascending (the
+ * symmetric neighbour set, FillAdjList's edge predicate of
+ * include/EditDistance.hpp:368-372 restated as igo_lev_myers). */
+typedef struct {
+    const uint32_t *words;
+    int32_t n;
+    int len, min_ed;
+    const int32_t *rows;
+    int32_t nrows;
+    int t, nthreads;
+    int32_t **out;
+    int64_t *cnt;
+    int fail;
+} row_job;
+
+static void *row_worker(void *arg)
+{
+    row_job *jb = (row_job *)arg;
+    for (int32_t k = jb->t; k < jb->nrows; k += jb->nthreads) {
+        const int32_t r = jb->rows[k];
+        int64_t cap = 1024, used = 0;
+        int32_t *buf = (int32_t *)malloc((size_t)cap * sizeof(int32_t));
+        if (!buf) {
+            jb->fail = 1;
+            return NULL;
+        }
+        for (int32_t c = 0; c < jb->n; c++) {
+            if (c == r || igo_lev_myers(jb->words[r], jb->words[c], jb->len) >= jb->min_ed)
+                continue;
+            if (used == cap) {
+                cap *= 2;
+                int32_t *nb = (int32_t *)realloc(buf, (size_t)cap * sizeof(int32_t));
+                if (!nb) {
+                    free(buf);
+                    jb->fail = 1;
+                    return NULL;
+                }
+                buf = nb;
+            }
+            buf[used++] = c;
+        }
+        jb->out[k] = buf;
+        jb->cnt[k] = used;
+    }
+    return NULL;
+}
+
+int igo_row_neighbours(const uint32_t *words, int32_t n, int len, int min_ed, const int32_t *rows, int32_t nrows,
+                       int threads, int64_t *ptr, int32_t **cols)
+{
+    *cols = NULL;
+    if (threads < 1)
+        threads = 1;
+    int32_t **out = (int32_t **)calloc((size_t)nrows + 1, sizeof(int32_t *));
+    int64_t *cnt = (int64_t *)calloc((size_t)nrows + 1, sizeof(int64_t));
+    row_job *jobs = (row_job *)calloc((size_t)threads, sizeof(row_job));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    int fail = !out || !cnt || !jobs || !tid;
+    if (!fail) {
+        for (int t = 0; t < threads; t++) {
+            jobs[t] = (row_job){words, n, len, min_ed, rows, nrows, t, threads, out, cnt, 0};
+            pthread_create(&tid[t], NULL, row_worker, &jobs[t]);
+        }
+        for (int t = 0; t < threads; t++) {
+            pthread_join(tid[t], NULL);
+            fail |= jobs[t].fail;
+        }
+    }
+    if (!fail) {
+        ptr[0] = 0;
+        for (int32_t k = 0; k < nrows; k++)
+            ptr[k + 1] = ptr[k] + cnt[k];
+        *cols = (int32_t *)malloc((size_t)(ptr[nrows] ? ptr[nrows] : 1) * sizeof(int32_t));
+        fail = *cols == NULL;
+        for (int32_t k = 0; k < nrows && !fail; k++)
+            memcpy(*cols + ptr[k], out[k], (size_t)cnt[k] * sizeof(int32_t));
+    }
+    if (out)
+        for (int32_t k = 0; k < nrows; k++)
+            free(out[k]);
+    free(out);
+    free(cnt);
+    free(jobs);
+    free(tid);
+    return fail ? -1 : 0;
+}
+
 /* ---------------- neighbour order of FillAdjList(T) ---------------- */
 
 void igo_adjacency(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads, int64_t *adj_ptr,

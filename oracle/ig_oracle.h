@@ -43,6 +43,11 @@ int igo_conflict_upper_alloc(const uint32_t *words, int32_t n, int len, int min_
                              int32_t **cols);
 void igo_free(void *p);
 
+/* Symmetric neighbour rows of the sampled vertices rows[0..nrows): row k's
+ * neighbours (ascending) are (*cols)[ptr[k] .. ptr[k+1]) (release with igo_free). */
+int igo_row_neighbours(const uint32_t *words, int32_t n, int len, int min_ed, const int32_t *rows, int32_t nrows,
+                       int threads, int64_t *ptr, int32_t **cols);
+
 /* Neighbour lists in the order src/SparseMat.cpp:599-609 builds them for a
  * FillAdjList run with `order_threads` threads (1 = fully sorted, which is also
  * the order AdjList::FromBinaryFile builds from a row-sorted edge file).

@@ -56,6 +56,9 @@ def lib():
         L.igo_conflict_upper_alloc.restype = ctypes.c_int
         L.igo_conflict_upper_alloc.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                _i64p, ctypes.POINTER(ctypes.c_void_p)]
+        L.igo_row_neighbours.restype = ctypes.c_int
+        L.igo_row_neighbours.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int32,
+                                         ctypes.c_int, _i64p, ctypes.POINTER(ctypes.c_void_p)]
         L.igo_free.restype = None
         L.igo_free.argtypes = [ctypes.c_void_p]
         L.igo_adjacency.restype = None
@@ -115,6 +118,22 @@ def conflict_upper(words, L: int, min_ed: int, threads: int | None = None):
     finally:
         lib().igo_free(buf)
     return row_ptr, cols
+
+
+def row_neighbours(words, L: int, min_ed: int, rows, threads: int | None = None):
+    """Symmetric neighbour sets of the sampled rows: list of ascending int32 arrays."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    threads = threads or max(1, len(os.sched_getaffinity(0)))
+    ptr = np.zeros(len(rows) + 1, np.int64)
+    buf = ctypes.c_void_p()
+    if lib().igo_row_neighbours(w, len(w), L, min_ed, rows, len(rows), threads, ptr, ctypes.byref(buf)) != 0:
+        raise MemoryError("oracle row_neighbours failed")
+    try:
+        flat = np.ctypeslib.as_array(ctypes.cast(buf, ctypes.POINTER(ctypes.c_int32)), shape=(max(int(ptr[-1]), 1),))
+        return [flat[ptr[k]:ptr[k + 1]].copy() for k in range(len(rows))]
+    finally:
+        lib().igo_free(buf)
 
 
 def adjacency(row_ptr, cols, n: int, order_threads: int = 1):
