@@ -185,6 +185,19 @@ ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, i
 /* Cancels queued jobs, finishes the running batch, joins the threads. */
 ig_status ig_server_destroy(ig_server *sv);
 
+/* ---- clustering: nearest-centre assignment ------------------------------ */
+/* For each of the n words, the index of the nearest of the k centres
+ * (Levenshtein distance, ties to the lowest index), written to
+ * assignment[0..n).  Replaces solve_assignments_cuda (src/gpu_cluster.py:
+ * 239-300: dense K x N uint8 distance matrix + host np.argmin), which
+ * RandomCluster::fit runs through system()
+ * (src/clustering/impl/random_cluster/RandomCluster.cpp:68-111).  words and
+ * centres are packed like ig_graph_build's input, all of length len;
+ * on_device = 1: words, centers and assignment are device pointers (cuda:
+ * device of ctx), 0: host pointers.  k >= 1 when n > 0; n <= 2^31 - 1. */
+ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k,
+                            int len, int on_device, int32_t *assignment);
+
 /* ---- one-call conveniences --------------------------------------------- */
 
 /* SolveIndependentSet (src/SparseMat.cpp:784-851): graph + greedy.

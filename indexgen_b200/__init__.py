@@ -3,7 +3,8 @@
 The compute lives in libindexgen_cuda.so (hand-written CUDA for sm_100a behind
 the C ABI of include/indexgen_cuda.h); this package is the Python host mirror
 of the reference's GPU path (src/cuda_edit_distance.py, src/gpu_graph_generator.py,
-SolveIndependentSet / VerifyDist of src/SparseMat.cpp, src/Utils.cpp).
+SolveIndependentSet / VerifyDist of src/SparseMat.cpp, src/Utils.cpp, and the
+nearest-centre assignment of src/gpu_cluster.py).
 """
 from .graph import (  # noqa: F401
     ConflictGraph,
@@ -11,6 +12,7 @@ from .graph import (  # noqa: F401
     IndexGenError,
     Server,
     apply_filters,
+    assign_centers,
     build_batch,
     build_conflict_graph,
     codebook_from_upper_csr,
@@ -18,8 +20,10 @@ from .graph import (  # noqa: F401
     default_context,
     fill_adj_list_gpu,
     pack_sequences,
+    random_cluster_fit,
     solve,
     solve_batch,
+    solve_assignments_cuda,
     solve_edit_distance_cuda,
     solve_independent_set,
     verify_dist,

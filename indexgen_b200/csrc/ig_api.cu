@@ -385,7 +385,8 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
     {
         ig::DeviceGuard dg(ctx->device);
         for (ig::DevBuf *b :
-             {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags, &ctx->adj_tmp})
+             {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags, &ctx->adj_tmp,
+              &ctx->jobs, &ctx->aux})
             if (b->ptr)
                 cudaFreeAsync(b->ptr, ctx->stream);
         cudaStreamSynchronize(ctx->stream);
@@ -731,6 +732,51 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     if (s == IG_OK && !host_ok)
         s = ig::set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
     return s;
+}
+
+ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k,
+                            int len, int on_device, int32_t *assignment)
+{
+    if (!ctx || n < 0 || k < 0 || len < 1 || len > IG_MAX_LEN)
+        return IG_ERR_INPUT;
+    if (n == 0)
+        return IG_OK;
+    if (!words || !assignment || k < 1 || !centers)
+        return ig::set_error(ctx, IG_ERR_INPUT, "assign: words, centers (k >= 1) and assignment are required");
+    if (n > INT32_MAX)
+        return ig::set_error(ctx, IG_ERR_CAPACITY, "assign: more than 2^31-1 words");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    cudaStream_t st = ctx->stream;
+    if (on_device) {
+        ig_status s = ig::assign_centers(ctx, words, n, centers, k, len, assignment);
+        if (s != IG_OK)
+            return s;
+        const cudaError_t e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? IG_OK : ig::cuda_error(ctx, e, "assign");
+    }
+    const uint32_t *d_words = nullptr;
+    ig_status s = ig::stage_words(ctx, words, (int32_t)n, 0, &d_words);
+    if (s != IG_OK)
+        return s;
+    const size_t cbytes = ((size_t)k * sizeof(uint32_t) + 255) & ~(size_t)255;
+    s = ig::ensure_buffer(ctx, ctx->aux, cbytes + (size_t)n * sizeof(int32_t), "assignment workspace");
+    if (s != IG_OK)
+        return s;
+    uint32_t *d_centres = static_cast<uint32_t *>(ctx->aux.ptr);
+    int32_t *d_out = reinterpret_cast<int32_t *>(static_cast<char *>(ctx->aux.ptr) + cbytes);
+    cudaError_t e = cudaMemcpyAsync(d_centres, centers, (size_t)k * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess)
+        return ig::cuda_error(ctx, e, "centre upload");
+    s = ig::assign_centers(ctx, d_words, n, d_centres, k, len, d_out);
+    if (s != IG_OK)
+        return s;
+    e = cudaMemcpyAsync(assignment, d_out, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? IG_OK : ig::cuda_error(ctx, e, "assignment download");
 }
 
 ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,

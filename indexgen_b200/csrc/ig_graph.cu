@@ -621,24 +621,27 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
             break;
         const JobDesc J = a.jobs[find_job_by_item(a.jobs, a.njobs, item)];
         // local item -> (band, segment): bands are grouped by their first
-        // segment g; a band of group g owns segments g..nseg-1.
+        // segment g; a band of group g owns segments g..nseg-1.  Every group
+        // before the last is full, so group g starts at item
+        // bands_per_seg * (g * nseg - g (g - 1) / 2); find g by bisection.
         const long long li = item - J.item_off;
         int band = 0, seg = 0;
         {
-            long long base = 0;
-            for (int g = 0; g < J.nseg; ++g) {
-                const int b_lo = g * J.bands_per_seg;
-                const int b_hi = min(b_lo + J.bands_per_seg, J.nbands);
-                const int per = J.nseg - g;
-                const long long cnt = (long long)max(b_hi - b_lo, 0) * per;
-                if (li < base + cnt) {
-                    const long long q = li - base;
-                    band = b_lo + (int)(q / per);
-                    seg = g + (int)(q % per);
-                    break;
-                }
-                base += cnt;
+            int lo = 0, hi = J.nseg - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                const long long b = (long long)J.bands_per_seg *
+                                    ((long long)mid * J.nseg - (long long)mid * (mid - 1) / 2);
+                if (b <= li)
+                    lo = mid;
+                else
+                    hi = mid - 1;
             }
+            const long long q =
+                li - (long long)J.bands_per_seg * ((long long)lo * J.nseg - (long long)lo * (lo - 1) / 2);
+            const int per = J.nseg - lo;
+            band = lo * J.bands_per_seg + (int)(q / per);
+            seg = lo + (int)(q % per);
         }
         dispatch_item(J.L, a, J, band, seg, tile, bar, parity, aborted,
                       std::make_integer_sequence<int, IG_MAX_LEN>{});

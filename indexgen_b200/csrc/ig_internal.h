@@ -80,7 +80,7 @@ struct Ctx {
     std::string last_error;
     int64_t launches = 0;
     // workspace
-    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs;
+    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs, aux;
     unsigned long long rec_capacity = 0;  // records that fit in `records`
     int pair_grid = 0;                    // persistent CTAs of the pair kernel
     // optional per-phase timing (IG_PHASE_*)
@@ -140,6 +140,10 @@ ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what);
 bool reserve_pool(Ctx *ctx, size_t bytes);
 // Symmetric CSR in the canonical neighbour order (ig_adjacency.cu).
 ig_status build_adjacency(Ctx *ctx, Graph *g);
+// Nearest-centre index of every word, device pointers, on the context stream
+// (ig_assign.cu).
+ig_status assign_centers(Ctx *ctx, const uint32_t *d_words, int64_t n, const uint32_t *d_centres, int32_t k, int len,
+                         int32_t *d_out);
 
 // Host greedy (ig_host.cpp).  Vertex ids in cols / adj are global; `base`
 // is subtracted to get the job-local ids the greedy works with and returns.

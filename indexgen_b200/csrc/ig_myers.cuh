@@ -85,10 +85,11 @@ __device__ __forceinline__ uint32_t imad(uint32_t a, uint32_t b, uint32_t c)
 // +1 boundary into row 0 of both lanes without a carry, Mh*2 brings 0 into row 0
 // of lane 1, and the new Pv has bit 15 clear because Xv has it set.
 template <int L>
-__device__ __forceinline__ void myers_two(uint32_t p01, uint32_t p23, const uint32_t (&sel)[16], uint32_t one,
-                                          uint32_t two, int lim, bool &h0, bool &h1)
+__device__ __forceinline__ void myers_two_vectors(uint32_t p01, uint32_t p23, const uint32_t (&sel)[16],
+                                                  uint32_t one, uint32_t two, uint32_t &pv, uint32_t &mv)
 {
-    uint32_t pv = 0x7fff7fffu, mv = 0u;
+    pv = 0x7fff7fffu;
+    mv = 0u;
 #pragma unroll
     for (int k = 0; k < L; ++k) {
         const uint32_t eq = __byte_perm(p01, p23, sel[k]);
@@ -102,19 +103,42 @@ __device__ __forceinline__ void myers_two(uint32_t p01, uint32_t p23, const uint
         pv = mh2 | ~(xv | ph2);
         mv = ph2 & xv & 0x7fff7fffu;
     }
+}
+
+// Hit flags ED < lim + L of the two columns.
+template <int L>
+__device__ __forceinline__ void myers_two(uint32_t p01, uint32_t p23, const uint32_t (&sel)[16], uint32_t one,
+                                          uint32_t two, int lim, bool &h0, bool &h1)
+{
+    uint32_t pv, mv;
+    myers_two_vectors<L>(p01, p23, sel, one, two, pv, mv);
     constexpr uint32_t M0 = (1u << L) - 1u;
     constexpr uint32_t M1 = M0 << 16;
     h0 = (__popc(pv & M0) - __popc(mv & M0)) < lim;
     h1 = (__popc(pv & M1) - __popc(mv & M1)) < lim;
 }
 
+// Exact distances of the two columns.
+template <int L>
+__device__ __forceinline__ void myers_two_dist(uint32_t p01, uint32_t p23, const uint32_t (&sel)[16], uint32_t one,
+                                               uint32_t two, int &d0, int &d1)
+{
+    uint32_t pv, mv;
+    myers_two_vectors<L>(p01, p23, sel, one, two, pv, mv);
+    constexpr uint32_t M0 = (1u << L) - 1u;
+    constexpr uint32_t M1 = M0 << 16;
+    d0 = L + __popc(pv & M0) - __popc(mv & M0);
+    d1 = L + __popc(pv & M1) - __popc(mv & M1);
+}
+
 // One-lane form (L = 16): bits >= 16 of Eq hold other masks' bytes; carries
 // and shifts only move upwards, so they never reach the pattern rows.
 template <int L>
-__device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint32_t (&sel)[8], uint32_t one,
-                                          uint32_t two, uint32_t hi, int lim)
+__device__ __forceinline__ void myers_one_vectors(uint32_t p01, uint32_t p23, const uint32_t (&sel)[8], uint32_t one,
+                                                  uint32_t two, uint32_t hi, uint32_t &pv, uint32_t &mv)
 {
-    uint32_t pv = 0xffffffffu, mv = 0u;
+    pv = 0xffffffffu;
+    mv = 0u;
 #pragma unroll
     for (int k = 0; k < L; ++k) {
         const uint32_t sw = (k & 1) ? __umulhi(sel[k >> 1], hi) : sel[k >> 1];
@@ -129,8 +153,26 @@ __device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint
         pv = mh2 | ~(xv | ph2);
         mv = ph2 & xv;
     }
+}
+
+template <int L>
+__device__ __forceinline__ bool myers_one(uint32_t p01, uint32_t p23, const uint32_t (&sel)[8], uint32_t one,
+                                          uint32_t two, uint32_t hi, int lim)
+{
+    uint32_t pv, mv;
+    myers_one_vectors<L>(p01, p23, sel, one, two, hi, pv, mv);
     constexpr uint32_t M = (L >= 32) ? 0xffffffffu : ((1u << L) - 1u);
     return (__popc(pv & M) - __popc(mv & M)) < lim;
+}
+
+template <int L>
+__device__ __forceinline__ int myers_one_dist(uint32_t p01, uint32_t p23, const uint32_t (&sel)[8], uint32_t one,
+                                              uint32_t two, uint32_t hi)
+{
+    uint32_t pv, mv;
+    myers_one_vectors<L>(p01, p23, sel, one, two, hi, pv, mv);
+    constexpr uint32_t M = (L >= 32) ? 0xffffffffu : ((1u << L) - 1u);
+    return L + __popc(pv & M) - __popc(mv & M);
 }
 
 // ---------------------------------------------------------------------------

@@ -12,6 +12,9 @@ Reference interface this mirrors (same names, argument meaning, errors):
                                               SolveIndependentSet, src/SparseMat.cpp:784-851
 * ``verify_dist(codebook, min_ed)``          VerifyDist GPU branch, src/Utils.cpp:203-288
 * ``apply_filters(words, L, ...)``           CandidateGenerator::applyFilters, src/CandidateGenerator.cpp:24-50
+* ``solve_assignments_cuda(vectors, centers, batch_size)``
+                                              src/gpu_cluster.py:239-300 (nearest centre, np.argmin ties)
+* ``random_cluster_fit(data, k, seed)``      RandomCluster::fit, src/clustering/impl/random_cluster/RandomCluster.cpp:42-136
 
 All device work goes through the C ABI; nothing here computes a distance.
 """
@@ -259,6 +262,29 @@ def count_conflicts(words, L: int, min_ed: int, ctx: Context | None = None) -> i
     return int(e.value)
 
 
+def assign_centers(words, centers, L: int, ctx: Context | None = None):
+    """Index of the nearest centre of every word (Levenshtein, ties to the
+    lowest index): int32 array, or a CUDA int32 tensor when the words are a
+    CUDA tensor (the centres are then moved to the same device)."""
+    ctx = ctx or default_context()
+    if hasattr(words, "data_ptr") and getattr(words, "is_cuda", False):
+        import torch
+
+        c = centers if getattr(centers, "is_cuda", False) else torch.as_tensor(
+            np.ascontiguousarray(centers, dtype=np.uint32).view(np.int32), device=words.device)
+        out = torch.empty(words.numel(), dtype=torch.int32, device=words.device)
+        check(lib().ig_assign_centers(ctx.handle, ctypes.c_void_p(words.data_ptr()), words.numel(),
+                                      ctypes.c_void_p(c.data_ptr()), c.numel(), int(L), 1,
+                                      ctypes.c_void_p(out.data_ptr())), "ig_assign_centers", ctx.handle)
+        return out
+    w = _words_array(words)
+    c = _words_array(centers)
+    out = np.zeros(max(len(w), 1), np.int32)
+    check(lib().ig_assign_centers(ctx.handle, ptr(w), len(w), ptr(c), len(c), int(L), 0, ptr(out)),
+          "ig_assign_centers", ctx.handle)
+    return out[: len(w)]
+
+
 def codebook_from_upper_csr(row_ptr, cols, n: int, order_threads: int = 1) -> np.ndarray:
     rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
     cl = np.ascontiguousarray(cols, dtype=np.int32)
@@ -407,6 +433,40 @@ def solve_edit_distance_cuda(strings, threshold, tile_size=16384, max_gpu_memory
         return g.adj_list()
 
 
+def solve_assignments_cuda(vectors, centers, batch_size=32768, ctx=None):
+    """Mirror of src/gpu_cluster.py:239-300: the nearest centre (np.argmin
+    order: lowest index on ties) of every vector, int32.  batch_size is
+    accepted for interface parity; the kernel needs no distance matrix."""
+    K, N = len(centers), len(vectors)
+    if N == 0 or K == 0:
+        return np.array([], dtype=np.int32)
+    vw, Lv, _ = pack_sequences(list(vectors))
+    cw, Lc, _ = pack_sequences(list(centers))
+    if Lv != Lc:
+        raise ValueError("Length mismatch between vectors and centers.")
+    return assign_centers(vw, cw, Lv, ctx)
+
+
+def random_cluster_fit(data, k: int, seed: int, ctx=None):
+    """RandomCluster::fit (src/clustering/impl/random_cluster/RandomCluster.cpp:
+    42-136): k distinct random candidates become the centres, every candidate
+    joins its nearest centre, clusters keep candidate order, empty clusters are
+    dropped.  The reference seeds its shuffle from std::random_device; here the
+    shuffle is numpy's, seeded, so runs repeat."""
+    data = list(data)
+    if not data:
+        return []
+    if k <= 0:
+        return [data]
+    kk = min(k, len(data))
+    idx = np.random.default_rng(seed).permutation(len(data))[:kk]
+    a = solve_assignments_cuda(data, [data[i] for i in idx], ctx=ctx)
+    clusters = [[] for _ in range(kk)]
+    for s, c in zip(data, a.tolist()):
+        clusters[c if 0 <= c < kk else 0].append(s)
+    return [c for c in clusters if c]
+
+
 def fill_adj_list_gpu(candidates, min_ed: int, ctx=None):
     """FillAdjListGPU: returns (ConflictGraph, matrixOnesNum)."""
     words, L, _ = pack_sequences(list(candidates))
@@ -440,5 +500,6 @@ __all__ = [
     "Context", "ConflictGraph", "IndexGenError", "Server", "build_conflict_graph", "build_batch", "solve_batch",
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
-    "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context",
+    "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
+    "solve_assignments_cuda", "random_cluster_fit",
 ]

@@ -215,6 +215,62 @@ static int conflict_upper_impl(const uint32_t *words, int32_t n, int len, int mi
     return fail ? -1 : 0;
 }
 
+/* ---------------- nearest-centre assignment ---------------- */
+/* solve_assignments_cuda (src/gpu_cluster.py:239-300): for each word the
+ * index of the centre at minimal Levenshtein distance, np.argmin order (the
+ * first, i.e. lowest, index on ties).  Distances by igo_lev_myers with the
+ * centre as the pattern, as the reference kernel builds Peq from the centres. */
+typedef struct {
+    const uint32_t *words, *centers;
+    int64_t n;
+    int32_t k;
+    int len, t, nthreads;
+    int32_t *out;
+} assign_job;
+
+static void *assign_worker(void *arg)
+{
+    assign_job *jb = (assign_job *)arg;
+    for (int64_t i = jb->t; i < jb->n; i += jb->nthreads) {
+        int best = 1 << 30;
+        int32_t arg_best = 0;
+        for (int32_t c = 0; c < jb->k; c++) {
+            const int d = igo_lev_myers(jb->centers[c], jb->words[i], jb->len);
+            if (d < best) {
+                best = d;
+                arg_best = c;
+            }
+        }
+        jb->out[i] = arg_best;
+    }
+    return NULL;
+}
+
+int igo_assign_centers(const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k, int len, int threads,
+                       int32_t *out)
+{
+    if (threads < 1)
+        threads = 1;
+    if (k < 1)
+        return n > 0 ? -1 : 0;
+    assign_job *jobs = (assign_job *)calloc((size_t)threads, sizeof(assign_job));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    if (!jobs || !tid) {
+        free(jobs);
+        free(tid);
+        return -1;
+    }
+    for (int t = 0; t < threads; t++) {
+        jobs[t] = (assign_job){words, centers, n, k, len, t, threads, out};
+        pthread_create(&tid[t], NULL, assign_worker, &jobs[t]);
+    }
+    for (int t = 0; t < threads; t++)
+        pthread_join(tid[t], NULL);
+    free(jobs);
+    free(tid);
+    return 0;
+}
+
 /* ---------------- full neighbour rows of sampled vertices ---------------- */
 /* For spot checks of graphs too large for the all-pairs oracle: for each
  * sampled row r, every c != r with ED(w_r, w_c) < min_ed, ascending (the

@@ -43,6 +43,10 @@ int igo_conflict_upper_alloc(const uint32_t *words, int32_t n, int len, int min_
                              int32_t **cols);
 void igo_free(void *p);
 
+/* Nearest centre of every word (Levenshtein; lowest index on ties). */
+int igo_assign_centers(const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k, int len, int threads,
+                       int32_t *out);
+
 /* Symmetric neighbour rows of the sampled vertices rows[0..nrows): row k's
  * neighbours (ascending) are (*cols)[ptr[k] .. ptr[k+1]) (release with igo_free). */
 int igo_row_neighbours(const uint32_t *words, int32_t n, int len, int min_ed, const int32_t *rows, int32_t nrows,

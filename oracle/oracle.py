@@ -59,6 +59,9 @@ def lib():
         L.igo_row_neighbours.restype = ctypes.c_int
         L.igo_row_neighbours.argtypes = [_u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int32,
                                          ctypes.c_int, _i64p, ctypes.POINTER(ctypes.c_void_p)]
+        L.igo_assign_centers.restype = ctypes.c_int
+        L.igo_assign_centers.argtypes = [_u32p, ctypes.c_int64, _u32p, ctypes.c_int32, ctypes.c_int, ctypes.c_int,
+                                         _i32p]
         L.igo_free.restype = None
         L.igo_free.argtypes = [ctypes.c_void_p]
         L.igo_adjacency.restype = None
@@ -134,6 +137,18 @@ def row_neighbours(words, L: int, min_ed: int, rows, threads: int | None = None)
         return [flat[ptr[k]:ptr[k + 1]].copy() for k in range(len(rows))]
     finally:
         lib().igo_free(buf)
+
+
+def assign_centers(words, centers, L: int, threads: int | None = None) -> np.ndarray:
+    """Nearest centre (Levenshtein, lowest index on ties) of every word."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    c = np.ascontiguousarray(centers, dtype=np.uint32)
+    threads = threads or max(1, len(os.sched_getaffinity(0)))
+    out = np.zeros(max(len(w), 1), np.int32)
+    if lib().igo_assign_centers(w if len(w) else np.zeros(1, np.uint32), len(w),
+                                c if len(c) else np.zeros(1, np.uint32), len(c), L, threads, out) != 0:
+        raise ValueError("oracle assign_centers failed")
+    return out[: len(w)]
 
 
 def adjacency(row_ptr, cols, n: int, order_threads: int = 1):

@@ -84,3 +84,32 @@ def test_n11_header_pin(oracle):
     rp, cols = oracle.conflict_upper(w, 11, 3)
     assert 2 * rp[-1] == 129128
     assert sha(oracle.pairs_from_csr(rp, cols).astype("<i4")) == info["edges_sha256"]
+
+
+def test_assignment_matches_reference(oracle):
+    """The oracle's nearest-centre assignment equals the reference's own
+    solve_assignments_cuda (src/gpu_cluster.py, run under Numba's CUDA
+    simulator by tests/golden/make_golden_assign.py), ties included."""
+    g = load_golden("assign.npz")
+    keys = sorted({k.rsplit("_", 1)[0] for k in g.files})
+    assert len(keys) == 10
+    for key in keys:
+        L = int(key.split("_")[0][1:])
+        got = oracle.assign_centers(g[key + "_words"], g[key + "_centers"], L)
+        assert np.array_equal(got, g[key + "_assign"]), key
+
+
+def test_row_neighbours_match_all_pairs(oracle):
+    from indexgen_b200 import workloads as W
+
+    w = W.uniform_words(2500, 10, 5)
+    rp, cols = oracle.conflict_upper(w, 10, 4)
+    full = [[] for _ in range(len(w))]
+    for i in range(len(w)):
+        for c in cols[rp[i]:rp[i + 1]]:
+            full[i].append(int(c))
+            full[int(c)].append(i)
+    rows = np.array([0, 7, 100, 1234, 2499], np.int32)
+    got = oracle.row_neighbours(w, 10, 4, rows)
+    for k, r in enumerate(rows):
+        assert sorted(full[int(r)]) == got[k].tolist(), int(r)
