@@ -198,6 +198,23 @@ ig_status ig_server_destroy(ig_server *sv);
 ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k,
                             int len, int on_device, int32_t *assignment);
 
+/* Iterative clustered solve with random_cluster, the words resident on the
+ * device (src/SparseMat.cpp:920-1095 with RandomCluster::fit,
+ * src/clustering/impl/random_cluster/RandomCluster.cpp:42-136): repeat
+ * {k random centres among the current candidates (k raised to
+ * ceil(N / 200000) when N / k > 200000; k <= 0: one cluster), nearest-centre
+ * clusters in candidate order, every cluster solved (greedy in the sorted
+ * neighbour order), codebooks concatenated in cluster order} until the last
+ * converge_iters codebook sizes agree (<= 1: after one iteration, < 0: never)
+ * or max_iters iterations ran.  codebook[0..*count) receives ids into words
+ * (room for n); sizes (optional, room for max_iters) the size after each
+ * iteration.  Centres come from a seeded splitmix64 partial Fisher-Yates
+ * shuffle (iteration t: seed ^ t * 0xD1B54A32D192ED03) where the reference
+ * draws from std::random_device. */
+ig_status ig_cluster_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int32_t k,
+                           int32_t converge_iters, uint64_t seed, int32_t max_iters, int host_threads,
+                           int32_t *codebook, int32_t *count, int32_t *iterations, int64_t *sizes);
+
 /* ---- one-call conveniences --------------------------------------------- */
 
 /* SolveIndependentSet (src/SparseMat.cpp:784-851): graph + greedy.

@@ -31,24 +31,6 @@ ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what)
 
 namespace {
 
-// Makes ctx->device current for the duration of a call and restores the
-// caller's device afterwards.
-struct DeviceGuard {
-    int prev = -1;
-    bool ok = false;
-    explicit DeviceGuard(int dev)
-    {
-        if (cudaGetDevice(&prev) != cudaSuccess)
-            prev = -1;
-        ok = cudaSetDevice(dev) == cudaSuccess;
-    }
-    ~DeviceGuard()
-    {
-        if (prev >= 0)
-            cudaSetDevice(prev);
-    }
-};
-
 ig_status check_job(const uint32_t *words, int32_t n, int len)
 {
     if (n < 0 || len < 1 || len > IG_MAX_LEN || (n > 0 && !words))

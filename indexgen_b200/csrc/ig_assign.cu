@@ -107,7 +107,25 @@ void launch_assign(int L, int grid, cudaStream_t st, const uint32_t *words, long
      ...);
 }
 
+__global__ void gather_words_kernel(const uint32_t *__restrict__ src, const int32_t *__restrict__ idx, long long n,
+                                    uint32_t *__restrict__ dst)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
 }  // namespace
+
+ig_status gather_words(Ctx *ctx, const uint32_t *d_src, const int32_t *d_idx, int64_t n, uint32_t *d_dst)
+{
+    if (n == 0)
+        return IG_OK;
+    const long long blocks = std::min<long long>((n + 255) / 256, (long long)ctx->sm_count * 8);
+    gather_words_kernel<<<(int)blocks, 256, 0, ctx->stream>>>(d_src, d_idx, n, d_dst);
+    ctx->launches++;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? IG_OK : cuda_error(ctx, e, "gather_words launch");
+}
 
 ig_status assign_centers(Ctx *ctx, const uint32_t *d_words, int64_t n, const uint32_t *d_centres, int32_t k, int len,
                          int32_t *d_out)

@@ -144,6 +144,8 @@ ig_status build_adjacency(Ctx *ctx, Graph *g);
 // (ig_assign.cu).
 ig_status assign_centers(Ctx *ctx, const uint32_t *d_words, int64_t n, const uint32_t *d_centres, int32_t k, int len,
                          int32_t *d_out);
+// d_dst[i] = d_src[d_idx[i]], i < n, on the context stream (ig_assign.cu).
+ig_status gather_words(Ctx *ctx, const uint32_t *d_src, const int32_t *d_idx, int64_t n, uint32_t *d_dst);
 
 // Host greedy (ig_host.cpp).  Vertex ids in cols / adj are global; `base`
 // is subtracted to get the job-local ids the greedy works with and returns.
@@ -170,6 +172,24 @@ ig_status download_for_greedy(Graph *g, int order_threads, HostGraph &hg);
 bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts);
 // Greedy of one job of a downloaded graph into out (job-local ids).
 int32_t greedy_one(const HostGraph &hg, int job, int32_t *out);
+
+// Makes a device current for the duration of a call and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int dev)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess)
+            prev = -1;
+        ok = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0)
+            cudaSetDevice(prev);
+    }
+};
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);

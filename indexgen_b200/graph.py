@@ -15,6 +15,7 @@ Reference interface this mirrors (same names, argument meaning, errors):
 * ``solve_assignments_cuda(vectors, centers, batch_size)``
                                               src/gpu_cluster.py:239-300 (nearest centre, np.argmin ties)
 * ``random_cluster_fit(data, k, seed)``      RandomCluster::fit, src/clustering/impl/random_cluster/RandomCluster.cpp:42-136
+* ``cluster_solve(words, L, min_ed, k, ...)`` the iterative clustered solve, src/SparseMat.cpp:920-1095
 
 All device work goes through the C ABI; nothing here computes a distance.
 """
@@ -467,6 +468,23 @@ def random_cluster_fit(data, k: int, seed: int, ctx=None):
     return [c for c in clusters if c]
 
 
+def cluster_solve(words, L: int, min_ed: int, k: int, converge_iters: int = 3, seed: int = 0,
+                  max_iters: int = 50, host_threads: int = 0, ctx: Context | None = None):
+    """Iterative clustered solve with random_cluster (src/SparseMat.cpp:920-1095)
+    with the words resident on the device: (codebook ids into words, sizes
+    after each iteration)."""
+    ctx = ctx or default_context()
+    w = _words_array(words)
+    book = np.zeros(max(len(w), 1), np.int32)
+    sizes = np.zeros(max(int(max_iters), 1), np.int64)
+    cnt = ctypes.c_int32()
+    it = ctypes.c_int32()
+    check(lib().ig_cluster_solve(ctx.handle, ptr(w), len(w), int(L), int(min_ed), int(k), int(converge_iters),
+                                 int(seed) & ((1 << 64) - 1), int(max_iters), int(host_threads), ptr(book),
+                                 ctypes.byref(cnt), ctypes.byref(it), ptr(sizes)), "ig_cluster_solve", ctx.handle)
+    return book[: cnt.value], sizes[: it.value]
+
+
 def fill_adj_list_gpu(candidates, min_ed: int, ctx=None):
     """FillAdjListGPU: returns (ConflictGraph, matrixOnesNum)."""
     words, L, _ = pack_sequences(list(candidates))
@@ -501,5 +519,5 @@ __all__ = [
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
-    "solve_assignments_cuda", "random_cluster_fit",
+    "solve_assignments_cuda", "random_cluster_fit", "cluster_solve",
 ]

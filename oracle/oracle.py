@@ -179,3 +179,63 @@ def pairs_from_csr(row_ptr, cols) -> np.ndarray:
     row_ptr = np.asarray(row_ptr, dtype=np.int64)
     rows = np.repeat(np.arange(len(row_ptr) - 1, dtype=np.int32), np.diff(row_ptr))
     return np.stack([rows, np.asarray(cols, dtype=np.int32)], axis=1)
+
+
+_M64 = (1 << 64) - 1
+
+
+def _splitmix64(state):
+    state = (state + 0x9E3779B97F4A7C15) & _M64
+    z = state
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _M64
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _M64
+    return state, z ^ (z >> 31)
+
+
+def pick_centres(n: int, k: int, seed: int, iteration: int) -> np.ndarray:
+    """First k entries of a splitmix64-driven partial Fisher-Yates shuffle of
+    range(n), state seed ^ iteration * 0xD1B54A32D192ED03 (the library's
+    stand-in for RandomCluster's std::random_device shuffle)."""
+    idx = np.arange(n, dtype=np.int64)
+    x = (seed ^ ((iteration * 0xD1B54A32D192ED03) & _M64)) & _M64
+    for i in range(k):
+        x, r = _splitmix64(x)
+        j = i + r % (n - i)
+        idx[i], idx[j] = idx[j], idx[i]
+    return idx[:k]
+
+
+def cluster_solve(words, L: int, min_ed: int, k: int, converge_iters: int = 3, seed: int = 0, max_iters: int = 50):
+    """The iterative clustered solve of src/SparseMat.cpp:920-1095 with
+    random_cluster (RandomCluster.cpp:42-136), restated on the oracle's
+    assignment, edge set and greedy: (codebook ids into words, sizes)."""
+    w = np.ascontiguousarray(words, dtype=np.uint32)
+    cur = np.arange(len(w), dtype=np.int64)
+    sizes = []
+    it = 0
+    while len(cur) and it < max_iters:
+        it += 1
+        N = len(cur)
+        eff_k = k
+        if eff_k > 0 and N // eff_k > 200000:
+            eff_k = max(2, (N + 199999) // 200000)
+        if eff_k > 0:
+            kk = min(eff_k, N)
+            cen = w[cur[pick_centres(N, kk, seed, it)]]
+            asg = assign_centers(w[cur], cen, L)
+        else:
+            kk = 1
+            asg = np.zeros(N, np.int32)
+        nxt = []
+        for c in range(kk):
+            members = cur[asg == c]
+            if len(members) == 0:
+                continue
+            rp, cols = conflict_upper(w[members], L, min_ed)
+            nxt.extend(members[codebook(rp, cols, len(members), 1)].tolist())
+        sizes.append(len(nxt))
+        cur = np.asarray(nxt, dtype=np.int64)
+        if converge_iters >= 0 and len(sizes) >= converge_iters and \
+                all(sizes[-1] == sizes[-1 - c] for c in range(1, converge_iters)):
+            break
+    return cur.astype(np.int32), np.asarray(sizes, np.int64)

@@ -113,3 +113,14 @@ def test_row_neighbours_match_all_pairs(oracle):
     got = oracle.row_neighbours(w, 10, 4, rows)
     for k, r in enumerate(rows):
         assert sorted(full[int(r)]) == got[k].tolist(), int(r)
+
+
+def test_cluster_oracle_single_cluster_is_plain_greedy(oracle):
+    from indexgen_b200 import workloads as W
+
+    w = W.uniform_until(1500, 10, 4)
+    book, sizes = oracle.cluster_solve(w, 10, 3, 0, converge_iters=1)
+    rp, cols = oracle.conflict_upper(w, 10, 3)
+    assert np.array_equal(book, oracle.codebook(rp, cols, len(w), 1)) and list(sizes) == [len(book)]
+    idx = oracle.pick_centres(100, 10, 7, 1)
+    assert len(set(idx.tolist())) == 10 and idx.min() >= 0 and idx.max() < 100
