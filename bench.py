@@ -283,6 +283,99 @@ def run_batch_section(ctx, reps: int = 3) -> dict:
             "note": "wall clock through solve_batch vs a loop of solve (graph + greedy per cluster)"}
 
 
+def run_assign_section(ctx, reps: int = 5) -> dict:
+    """random_cluster's assignment step (src/gpu_cluster.py): 1,000,000
+    filtered uniform n=14 words against 64 seeded random centres, nearest
+    centre each.  Device rate (words resident, CUDA events on the library
+    stream), end to end with host buffers, and the C oracle on all host cores
+    on a 20,000-word sample of the same job (results compared)."""
+    import ctypes
+
+    import torch
+
+    from indexgen_b200 import assign_centers
+    from indexgen_b200._lib import check, lib
+    from oracle import oracle as O
+
+    L, K = 14, 64
+    w = W.uniform_until(1_000_000, L, 14, max_run=3, min_gc=0.3, max_gc=0.7)
+    c = w[np.random.default_rng(64).choice(len(w), K, replace=False)]
+    dw = torch.from_numpy(w.view(np.int32)).cuda()
+    dc = torch.from_numpy(c.view(np.int32)).cuda()
+    out = torch.empty(len(w), dtype=torch.int32, device="cuda")
+    ext = torch.cuda.ExternalStream(ctx.stream)
+
+    def dev_call():
+        check(lib().ig_assign_centers(ctx.handle, ctypes.c_void_p(dw.data_ptr()), len(w),
+                                      ctypes.c_void_p(dc.data_ptr()), K, L, 1, ctypes.c_void_p(out.data_ptr())),
+              "ig_assign_centers", ctx.handle)
+
+    for _ in range(3):
+        dev_call()
+    ms = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        dev_call()
+        e1.record(ext)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    dist = len(w) * K
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        host = assign_centers(w, c, L, ctx)
+    e2e_s = (time.perf_counter() - t0) / reps
+    sample = w[:20000]
+    t0 = time.perf_counter()
+    ref = O.assign_centers(sample, c, L)
+    cpu_s = time.perf_counter() - t0
+    same = bool(np.array_equal(ref, host[:20000]) and np.array_equal(out.cpu().numpy(), host))
+    alu_ops = 4 * L  # two-lane Myers: 7 LOP3 + 1 PRMT per step for two distances
+    peaks, _ = measured_peaks()
+    dev_s = min(ms) / 1e3
+    alu_peak = torch.cuda.get_device_properties(0).multi_processor_count * 64 * float(
+        peaks.get("sm_max_mhz", 1965.0)) * 1e6
+    return {"workload": "1,000,000 filtered uniform n=14 words, 64 random centres (seed 64)",
+            "distances": dist, "device_gdist_per_s": dist / dev_s / 1e9, "device_ms": dev_s * 1e3,
+            "e2e_gdist_per_s": dist / e2e_s / 1e9, "e2e_ms": e2e_s * 1e3,
+            "roofline": {"bound": "int32-alu-pipe", "alu_ops_per_distance": alu_ops,
+                         "frac": dist * alu_ops / dev_s / alu_peak},
+            "cpu_oracle_gdist_per_s": len(sample) * K / cpu_s / 1e9, "cpu_cores": host_cores(),
+            "identical_to_oracle": same}
+
+
+def run_cluster_section(ctx) -> dict:
+    """The iterative clustered solve (src/SparseMat.cpp:920-1095, random_cluster):
+    200,000 filtered uniform n=12 words, editDist 4, k = 16, two iterations,
+    resident on the device (ig_cluster_solve) against the plain flow of the
+    same iterations (assignment with host buffers, then one ig_solve call per
+    cluster), same centres; both must give the same codebook."""
+    from indexgen_b200 import assign_centers, cluster_centres, cluster_solve, solve
+
+    L, d, k, iters = 12, 4, 16, 2
+    w = W.uniform_until(200_000, L, 1212, max_run=3, min_gc=0.3, max_gc=0.7)
+    cluster_solve(w, L, d, k, converge_iters=-1, seed=5, max_iters=1, ctx=ctx)  # warm-up
+    t0 = time.perf_counter()
+    book, sizes = cluster_solve(w, L, d, k, converge_iters=-1, seed=5, max_iters=iters, ctx=ctx)
+    t_res = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cur = np.arange(len(w))
+    for it in range(1, iters + 1):
+        cen = w[cur[cluster_centres(len(cur), min(k, len(cur)), 5, it)]]
+        asg = assign_centers(w[cur], cen, L, ctx)
+        nxt = []
+        for cidx in range(min(k, len(cur))):
+            members = cur[asg == cidx]
+            if len(members):
+                nxt.extend(members[solve(w[members], L, d, 1, ctx)[0]].tolist())
+        cur = np.asarray(nxt)
+    t_plain = time.perf_counter() - t0
+    return {"workload": "200,000 filtered uniform n=12 words, editDist 4, k=16 random centres, 2 iterations",
+            "resident_s": t_res, "plain_s": t_plain, "speedup": t_plain / t_res,
+            "sizes": [int(x) for x in sizes], "identical_to_plain": bool(np.array_equal(book, cur))}
+
+
 def run_serve_section(ctx, jobs: int, nmax: int, rate: float = 50.0) -> dict:
     """Serving stream: seeded Poisson arrivals (mean `rate` jobs/s), n uniform
     in 10..16, editDist uniform in 3..5, candidates log-uniform in [5k, nmax].
@@ -499,6 +592,8 @@ def run_ours(args, wl, rank, world, dist):
     }
     if not args.no_batch:
         line["batch"] = run_batch_section(ctx)
+        line["assign"] = run_assign_section(ctx)
+        line["cluster"] = run_cluster_section(ctx)
     if args.serve_jobs > 0:
         line["serve"] = run_serve_section(ctx, args.serve_jobs, args.serve_nmax)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

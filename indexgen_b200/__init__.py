@@ -15,6 +15,7 @@ from .graph import (  # noqa: F401
     assign_centers,
     build_batch,
     build_conflict_graph,
+    cluster_centres,
     cluster_solve,
     codebook_from_upper_csr,
     count_conflicts,

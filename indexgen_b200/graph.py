@@ -468,6 +468,25 @@ def random_cluster_fit(data, k: int, seed: int, ctx=None):
     return [c for c in clusters if c]
 
 
+def cluster_centres(n: int, k: int, seed: int, iteration: int) -> np.ndarray:
+    """Indices (into the current candidates) of the centres ig_cluster_solve
+    takes in iteration `iteration` (1-based): the first k entries of a
+    splitmix64-driven partial Fisher-Yates shuffle of range(n), state
+    seed ^ iteration * 0xD1B54A32D192ED03."""
+    m64 = (1 << 64) - 1
+    idx = np.arange(n, dtype=np.int64)
+    x = (int(seed) ^ ((int(iteration) * 0xD1B54A32D192ED03) & m64)) & m64
+    for i in range(int(k)):
+        x = (x + 0x9E3779B97F4A7C15) & m64
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m64
+        z ^= z >> 31
+        j = i + z % (n - i)
+        idx[i], idx[j] = idx[j], idx[i]
+    return idx[:k]
+
+
 def cluster_solve(words, L: int, min_ed: int, k: int, converge_iters: int = 3, seed: int = 0,
                   max_iters: int = 50, host_threads: int = 0, ctx: Context | None = None):
     """Iterative clustered solve with random_cluster (src/SparseMat.cpp:920-1095)
@@ -519,5 +538,5 @@ __all__ = [
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
-    "solve_assignments_cuda", "random_cluster_fit", "cluster_solve",
+    "solve_assignments_cuda", "random_cluster_fit", "cluster_solve", "cluster_centres",
 ]

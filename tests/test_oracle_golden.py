@@ -124,3 +124,10 @@ def test_cluster_oracle_single_cluster_is_plain_greedy(oracle):
     assert np.array_equal(book, oracle.codebook(rp, cols, len(w), 1)) and list(sizes) == [len(book)]
     idx = oracle.pick_centres(100, 10, 7, 1)
     assert len(set(idx.tolist())) == 10 and idx.min() >= 0 and idx.max() < 100
+
+
+def test_library_centre_picker_matches_oracle(oracle):
+    from indexgen_b200 import cluster_centres
+
+    for n, k, seed, it in ((100, 10, 7, 1), (5000, 64, 2**63 + 5, 3), (17, 17, 0, 2)):
+        assert np.array_equal(cluster_centres(n, k, seed, it), oracle.pick_centres(n, k, seed, it))
