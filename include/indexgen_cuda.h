@@ -185,6 +185,20 @@ ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, i
 /* Cancels queued jobs, finishes the running batch, joins the threads. */
 ig_status ig_server_destroy(ig_server *sv);
 
+/* ---- checkpoint bridge --------------------------------------------------- */
+/* Writes the graph as the reference's progress_adj_list.txt: AdjList::ToFile
+ * (src/SparseMat.cpp:286-305, SaveProgressCodebook :658-663) of the AdjList
+ * the GPU edge file loads into (FromBinaryFile, :338-390), i.e. "i\tj\n" for
+ * every neighbour j of every row i, rows ascending, lower neighbours then
+ * upper neighbours ascending.  The text is formatted on the device.  bytes
+ * (optional) = file size. */
+ig_status ig_graph_write_adj_list(ig_graph *g, const char *path, int64_t *bytes);
+/* Reads such a file (also one written part-way through the greedy, with the
+ * deleted rows gone) into a graph, as AdjList::FromFile (:306-336) does: n =
+ * largest id + 1, each row's neighbours in file order, which the codebook
+ * greedy then walks (ig_graph_codebook with order_threads = 1). */
+ig_status ig_graph_read_adj_list(ig_ctx *ctx, const char *path, ig_graph **out);
+
 /* ---- clustering: nearest-centre assignment ------------------------------ */
 /* For each of the n words, the index of the nearest of the k centres
  * (Levenshtein distance, ties to the lowest index), written to

@@ -23,6 +23,7 @@ from .graph import (  # noqa: F401
     fill_adj_list_gpu,
     pack_sequences,
     random_cluster_fit,
+    read_adj_list,
     solve,
     solve_batch,
     solve_assignments_cuda,

@@ -20,7 +20,7 @@ EXPORTS = (
     "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_adjacency",
     "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
-    "ig_assign_centers", "ig_cluster_solve",
+    "ig_assign_centers", "ig_cluster_solve", "ig_graph_write_adj_list", "ig_graph_read_adj_list",
     "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_codebooks", "ig_solve_batch",
     "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
     "ig_server_stats", "ig_server_destroy",
@@ -82,6 +82,8 @@ def _declare(L):
         "ig_codebook_from_upper_csr": (_int, [_vp, _vp, _i32, _int, _vp, ctypes.POINTER(_i32)]),
         "ig_count_conflicts_noalloc": (_int, [_vp, _i32, _int, _int, _vp, _vp]),
         "ig_assign_centers": (_int, [_vp, _vp, _i64, _vp, _i32, _int, _int, _vp]),
+        "ig_graph_write_adj_list": (_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_i64)]),
+        "ig_graph_read_adj_list": (_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp)]),
         "ig_cluster_solve": (_int, [_vp, _vp, _i32, _int, _int, _i32, _i32, ctypes.c_uint64, _i32, _int, _vp,
                                     ctypes.POINTER(_i32), ctypes.POINTER(_i32), _vp]),
         "ig_batch_build": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, ctypes.POINTER(_vp)]),

@@ -716,6 +716,39 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     return s;
 }
 
+ig_status ig_graph_write_adj_list(ig_graph *g, const char *path, int64_t *bytes)
+{
+    if (!g || !path)
+        return IG_ERR_INPUT;
+    ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    return ig::write_adj_list(ctx, g, path, bytes);
+}
+
+ig_status ig_graph_read_adj_list(ig_ctx *ctx, const char *path, ig_graph **out)
+{
+    if (!ctx || !path || !out)
+        return IG_ERR_INPUT;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    ig_graph *g = new (std::nothrow) ig_graph();
+    if (!g)
+        return IG_ERR_OOM;
+    const ig_status s = ig::read_adj_list(ctx, path, g);
+    if (s != IG_OK) {
+        ig::release_graph(g);
+        return s;
+    }
+    *out = g;
+    return IG_OK;
+}
+
 ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k,
                             int len, int on_device, int32_t *assignment)
 {

@@ -144,6 +144,9 @@ ig_status build_adjacency(Ctx *ctx, Graph *g);
 // (ig_assign.cu).
 ig_status assign_centers(Ctx *ctx, const uint32_t *d_words, int64_t n, const uint32_t *d_centres, int32_t k, int len,
                          int32_t *d_out);
+// progress_adj_list.txt (AdjList::ToFile format) from / to a graph (ig_progress.cu).
+ig_status write_adj_list(Ctx *ctx, Graph *g, const char *path, int64_t *bytes);
+ig_status read_adj_list(Ctx *ctx, const char *path, Graph *g);
 // d_dst[i] = d_src[d_idx[i]], i < n, on the context stream (ig_assign.cu).
 ig_status gather_words(Ctx *ctx, const uint32_t *d_src, const int32_t *d_idx, int64_t n, uint32_t *d_dst);
 

@@ -22,6 +22,7 @@ All device work goes through the C ABI; nothing here computes a distance.
 from __future__ import annotations
 
 import ctypes
+import os
 import threading
 
 import numpy as np
@@ -175,6 +176,14 @@ class ConflictGraph:
             out.append(order[f:f + counts[j]].copy())
         return out
 
+    def write_adj_list(self, path) -> int:
+        """Write the reference's progress_adj_list.txt for this graph
+        (AdjList::ToFile format); returns the file size in bytes."""
+        b = ctypes.c_int64()
+        check(lib().ig_graph_write_adj_list(self.handle, os.fsencode(path), ctypes.byref(b)),
+              "ig_graph_write_adj_list", self.ctx.handle)
+        return int(b.value)
+
     def adj_list(self):
         """Neighbour lists in both directions, ascending (list of lists)."""
         adj_ptr, adj = self.adjacency()
@@ -252,6 +261,16 @@ def solve_batch(jobs, order_threads: int = 1, host_threads: int = 0, ctx: Contex
                                int(host_threads), ptr(order), ptr(counts), ptr(edges)), "ig_solve_batch",
           ctx.handle)
     return [order[offsets[j]:offsets[j] + counts[j]].copy() for j in range(k)], edges[:k].copy()
+
+
+def read_adj_list(path, ctx: Context | None = None) -> ConflictGraph:
+    """A graph from a progress_adj_list.txt (AdjList::FromFile semantics: n =
+    largest id + 1, neighbours in file order)."""
+    ctx = ctx or default_context()
+    h = ctypes.c_void_p()
+    check(lib().ig_graph_read_adj_list(ctx.handle, os.fsencode(path), ctypes.byref(h)), "ig_graph_read_adj_list",
+          ctx.handle)
+    return ConflictGraph(h, ctx, 0, 0)
 
 
 def count_conflicts(words, L: int, min_ed: int, ctx: Context | None = None) -> int:
@@ -538,5 +557,5 @@ __all__ = [
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
-    "solve_assignments_cuda", "random_cluster_fit", "cluster_solve", "cluster_centres",
+    "solve_assignments_cuda", "random_cluster_fit", "cluster_solve", "cluster_centres", "read_adj_list",
 ]

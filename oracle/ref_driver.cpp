@@ -139,6 +139,47 @@ int main(int argc, char **argv)
         cout << "{\"N\": " << N << ", \"ones\": " << ones << ", \"codebook\": " << sel.size() << "}" << endl;
         return 0;
     }
+    if (cmd == "tofile" && argc == 5)
+    {
+        // progress_adj_list.txt as the GPU path writes it: AdjList::Init +
+        // FromBinaryFile of the pair file, then AdjList::ToFile (the first
+        // SaveProgressCodebook of Codebook).  argv[2] = N, argv[3] = pair
+        // file, argv[4] = output text.
+        int N = atoi(argv[2]);
+        AdjList adj;
+        long long ones = 0;
+        adj.Init(N);
+        adj.FromBinaryFile(argv[3], ones, true);
+        adj.ToFile(argv[4]);
+        cout << "{\"N\": " << N << ", \"ones\": " << ones << "}" << endl;
+        return 0;
+    }
+    if (cmd == "resume" && argc == 5)
+    {
+        // Codebook from a progress_adj_list.txt with every candidate still
+        // remaining: AdjList::FromFile, the degree buckets (RowsBySum, which
+        // the resume path needs before FindMinDel), the FindMinDel loop, then
+        // the remaining candidates in id order.  argv[2] = candidate count N,
+        // argv[3] = text file, argv[4] = output.
+        int N = atoi(argv[2]);
+        AdjList adj;
+        adj.FromFile(argv[3]);
+        adj.RowsBySum();
+        vector<bool> remaining(N, true);
+        double d1 = 0, d2 = 0;
+        vector<int32_t> sel;
+        while (!adj.empty())
+            sel.push_back(adj.FindMinDel(remaining, d1, d2));
+        for (int i = 0; i < N; i++)
+            if (remaining[i])
+                sel.push_back(i);
+        vector<int32_t> out;
+        out.push_back((int32_t)sel.size());
+        out.insert(out.end(), sel.begin(), sel.end());
+        write_i32(argv[4], out);
+        cout << "{\"N\": " << N << ", \"codebook\": " << sel.size() << "}" << endl;
+        return 0;
+    }
     if (argc < 5)
     {
         cerr << "bad arguments\n";
