@@ -222,13 +222,13 @@ def profile_traffic(wl_name):
 
 def alu_ops_per_pair(L: int, d: int) -> float:
     """ALU-pipe operations (LOP3 + PRMT) the pair-test recurrence issues per
-    pair test, counted from the kernel source: the banded 8-lane form takes 10
-    per character step for 8 pairs plus 2 per nibble-counter flush (every 7
-    steps and at the end) and 2 for the threshold (editDist <= 4); the 4-lane
-    form 9 per step for 4 pairs plus 1 (editDist 5..8); full Myers 8 per step
-    for 2 pairs (L <= 15) or for 1."""
+    pair test, counted from the kernel source: the banded 8-lane form (two
+    rows x four columns) takes 9 per character step for 8 pairs plus 2 per
+    nibble-counter flush (every 7 steps and at the end) and 2 for the
+    threshold (editDist <= 4); the 4-lane form 9 per step for 4 pairs plus 1
+    (editDist 5..8); full Myers 8 per step for 2 pairs (L <= 15) or for 1."""
     if 1 <= d <= 4:
-        return (10.0 * L + 2 * -(-L // 7) + 2) / 8
+        return (9.0 * L + 2 * -(-L // 7) + 2) / 8
     if 5 <= d <= 8:
         return (9.0 * L + 1) / 4
     return 8.0 / 2 * L if L <= 15 else 8.0 * L

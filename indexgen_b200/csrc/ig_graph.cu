@@ -13,9 +13,10 @@
 //                   per thread, keep their match masks in registers; column tiles
 //                   of the segment are staged into shared memory by cp.async.bulk
 //                   (TMA bulk copy, no multicast) with a two-slot mbarrier
-//                   pipeline; each thread tests its row against 8 (banded nibble
-//                   lanes, editDist <= 4), 4 (byte lanes, editDist <= 8) or 2/1
-//                   (full Myers) columns per 32-bit word and emits hits as
+//                   pipeline; each thread tests its row against 4 (byte lanes,
+//                   editDist 5..8) or 2/1 (full Myers) columns per 32-bit word
+//                   (pair_kernel_nib: two rows against 4 columns, nibble lanes,
+//                   editDist <= 4, 128 threads per band) and emits hits as
 //                   (row, col, rank-in-(row,segment), cell) records into slots
 //                   its warp takes in chunks, plus a per-(row, segment) count.
 //   row_prefix      per-row exclusive prefix over its segments + degree
@@ -151,21 +152,19 @@ __global__ void prep_units(const uint32_t *__restrict__ words, const JobDesc *__
     const uint32_t *w = words + J.word_off;
     uint4 *out = units + J.unit_off;
     if (J.mode == kModeNib) {
-        // 8 columns; word j: columns 0,2,4,6 in bits 0..15, 1,3,5,7 in 16..31
-        uint32_t cw[8];
+        // 4 columns; word j: nibble l = char of column l at position j
+        uint32_t cw[4];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-            cw[c] = (8 * p + c < J.n) ? w[8 * p + c] : 0u;
+        for (int c = 0; c < 4; ++c)
+            cw[c] = (4 * p + c < J.n) ? w[4 * p + c] : 0u;
         uint32_t o[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             uint32_t x = 0u;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                x |= ((cw[2 * m] >> (2 * j)) & 3u) << (4 * m);
-                x |= ((cw[2 * m + 1] >> (2 * j)) & 3u) << (16 + 4 * m);
-            }
-            o[j] = x;
+            for (int l = 0; l < 4; ++l)
+                x |= ((cw[l] >> (2 * j)) & 3u) << (4 * l);
+            o[j] = (j < J.L) ? x : 0u;
         }
 #pragma unroll
         for (int v = 0; v < 4; ++v)
@@ -225,7 +224,6 @@ struct PairArgs {
     uint32_t hi;
     uint32_t h28;
     uint32_t h31;
-    uint32_t c16;
     unsigned long long *work;
     unsigned long long *rec_count;  // record slots handed out (chunks of kSlotChunk)
     unsigned long long *hit_count;  // pair tests that are edges (exact)
@@ -396,62 +394,37 @@ __device__ __forceinline__ void tile_pass(const PairArgs &a, const uint4 *tile, 
     }
 }
 
-// Banded forms: one unit = 8 (kNib) or 4 (kByte) columns.
+// Byte lanes (editDist 5..8): one unit = 4 columns against the thread's row.
 template <int L, int MODE, bool CHECK>
 __device__ __forceinline__ void tile_pass_band(const PairArgs &a, const uint4 *tile, int nu, int32_t c0,
                                                const RowCtx &r, const uint32_t (&W)[L], const BandConst &q,
                                                uint32_t &rank, int lane)
 {
+    static_assert(MODE == kModeByte, "the nibble form runs in pair_kernel_nib");
     using BU = BandUnit<MODE>;
     for (int u = 0; u < nu; ++u) {
         const uint4 *src = tile + u * BU::kVec;
-        uint32_t he, ho;
-        if constexpr (MODE == kModeNib) {
-            uint32_t sel[16];
+        uint32_t sel[8];
 #pragma unroll
-            for (int v = 0; v < 4; ++v) {
-                if (4 * v < L) {
-                    const uint4 t4 = src[v];
-                    sel[4 * v] = t4.x;
-                    sel[4 * v + 1] = t4.y;
-                    sel[4 * v + 2] = t4.z;
-                    sel[4 * v + 3] = t4.w;
-                } else {
-                    sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
-                }
+        for (int v = 0; v < 2; ++v) {
+            if (8 * v < L) {
+                const uint4 t4 = src[v];
+                sel[4 * v] = t4.x;
+                sel[4 * v + 1] = t4.y;
+                sel[4 * v + 2] = t4.z;
+                sel[4 * v + 3] = t4.w;
+            } else {
+                sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
             }
-            myers::band_nib<L>(W, sel, q, he, ho);
-        } else {
-            uint32_t sel[8];
-#pragma unroll
-            for (int v = 0; v < 2; ++v) {
-                if (8 * v < L) {
-                    const uint4 t4 = src[v];
-                    sel[4 * v] = t4.x;
-                    sel[4 * v + 1] = t4.y;
-                    sel[4 * v + 2] = t4.z;
-                    sel[4 * v + 3] = t4.w;
-                } else {
-                    sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
-                }
-            }
-            he = myers::band_byte<L>(W, sel, q);
-            ho = 0u;
         }
-        if (__any_sync(kFull, (he | ho) != 0u)) {
+        const uint32_t he = myers::band_byte<L>(W, sel, q);
+        if (__any_sync(kFull, he != 0u)) {
             const int32_t base_col = c0 + u * BU::kCols;
-            // hit flags sit at bits 8q+7: he of column 2q (kNib) or q (kByte), ho of column 2q+1
-            uint32_t m = 0u;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (MODE == kModeNib)
-                    m |= (((he >> (8 * q + 7)) & 1u) << (2 * q)) | (((ho >> (8 * q + 7)) & 1u) << (2 * q + 1));
-                else
-                    m |= ((he >> (8 * q + 7)) & 1u) << q;
-            }
+            // hit flag of column q at bit 8q+7
+            uint32_t m = ((he >> 7) & 1u) | ((he >> 14) & 2u) | ((he >> 21) & 4u) | ((he >> 28) & 8u);
             if (CHECK)
                 m &= upper_mask<BU::kCols>(r, base_col);
-            if (__any_sync(kFull, m != 0u))
+            if (!CHECK || __any_sync(kFull, m != 0u))
                 emit_mask<BU::kCols>(a, m, r, base_col, rank, lane);
         }
     }
@@ -499,7 +472,6 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
         q.c = J.cmask;
         q.k = J.kthr;
         q.one = a.one;
-        q.c16 = a.c16;
         q.h16 = a.hi;
         q.h28 = a.h28;
         q.h31 = a.h31;
@@ -576,9 +548,7 @@ __device__ __forceinline__ void dispatch_mode(int mode, const PairArgs &a, const
                                               uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
                                               bool &aborted)
 {
-    if (mode == kModeNib)
-        run_item<L, kModeNib>(a, J, band, seg, tile, bar, parity, aborted);
-    else if (mode == kModeByte)
+    if (mode == kModeByte)
         run_item<L, kModeByte>(a, J, band, seg, tile, bar, parity, aborted);
     else
         run_item<L, kModeFull>(a, J, band, seg, tile, bar, parity, aborted);
@@ -592,6 +562,82 @@ __device__ __forceinline__ void dispatch_item(int L, const PairArgs &a, const Jo
     ((L == Ls + 1 ? dispatch_mode<Ls + 1>(J.mode, a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
 }
 
+// Local item -> (band, segment): bands are grouped by their first segment g;
+// a band of group g owns segments g..nseg-1.  Every group before the last is
+// full, so group g starts at item bands_per_seg * (g * nseg - g (g - 1) / 2);
+// g is found by bisection.
+__device__ __forceinline__ void decode_item(const JobDesc &J, long long li, int &band, int &seg)
+{
+    int lo = 0, hi = J.nseg - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const long long b = (long long)J.bands_per_seg * ((long long)mid * J.nseg - (long long)mid * (mid - 1) / 2);
+        if (b <= li)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const long long q = li - (long long)J.bands_per_seg * ((long long)lo * J.nseg - (long long)lo * (lo - 1) / 2);
+    const int per = J.nseg - lo;
+    band = lo * J.bands_per_seg + (int)(q / per);
+    seg = lo + (int)(q % per);
+}
+
+// The unused rest of each warp's record-slot chunk becomes sentinels.
+__device__ __forceinline__ void fill_slot_tails(const PairArgs &a)
+{
+    const int tid = threadIdx.x;
+    const unsigned long long base = g_slot_base[tid >> 5];
+    const unsigned left = g_slot_left[tid >> 5];
+    for (unsigned k = tid & 31; k < left; k += 32) {
+        const unsigned long long idx = base + k;
+        if (idx < a.rec_cap)
+            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(kNoRow, 0u, 0u, 0u);
+    }
+}
+
+// Persistent item loop of the nibble-lane kernel: the CTA takes (job, band,
+// segment) items of its job table from its work counter and runs them.
+template <typename RunItem>
+__device__ __forceinline__ void item_loop(const PairArgs &a, uint64_t *bar, long long &item_sh, RunItem &&run_one)
+{
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    if ((tid & 31) == 0) {
+        g_slot_base[tid >> 5] = 0ull;
+        g_slot_left[tid >> 5] = 0u;
+    }
+    __syncthreads();
+    uint32_t parity = 0u;  // bit b: phase parity of slot b
+    bool aborted = false;
+
+    for (;;) {
+        if (tid == 0)
+            item_sh = (long long)atomicAdd(a.work, 1ull);
+        __syncthreads();
+        const long long item = item_sh;
+        if (item >= a.items || aborted)
+            break;
+        const JobDesc J = a.jobs[find_job_by_item(a.jobs, a.njobs, item)];
+        int band = 0, seg = 0;
+        decode_item(J, item - J.item_off, band, seg);
+        run_one(J, band, seg, parity, aborted);
+        if (aborted)
+            break;
+        __syncthreads();
+    }
+    if (a.emit && !aborted)
+        fill_slot_tails(a);
+}
+
+// Full-Myers and byte-lane jobs: one row per thread, 256 threads per band.
+// (The item loop is written out here rather than shared with
+// pair_kernel_nib: through the shared template this kernel's register
+// allocation got a 256-byte stack frame and ran 9 % slower.)
 __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
 {
     __shared__ __align__(128) uint4 tile[2][kSlotVec];
@@ -620,45 +666,224 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
         if (item >= a.items || aborted)
             break;
         const JobDesc J = a.jobs[find_job_by_item(a.jobs, a.njobs, item)];
-        // local item -> (band, segment): bands are grouped by their first
-        // segment g; a band of group g owns segments g..nseg-1.  Every group
-        // before the last is full, so group g starts at item
-        // bands_per_seg * (g * nseg - g (g - 1) / 2); find g by bisection.
-        const long long li = item - J.item_off;
         int band = 0, seg = 0;
-        {
-            int lo = 0, hi = J.nseg - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                const long long b = (long long)J.bands_per_seg *
-                                    ((long long)mid * J.nseg - (long long)mid * (mid - 1) / 2);
-                if (b <= li)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            const long long q =
-                li - (long long)J.bands_per_seg * ((long long)lo * J.nseg - (long long)lo * (lo - 1) / 2);
-            const int per = J.nseg - lo;
-            band = lo * J.bands_per_seg + (int)(q / per);
-            seg = lo + (int)(q % per);
-        }
+        decode_item(J, item - J.item_off, band, seg);
         dispatch_item(J.L, a, J, band, seg, tile, bar, parity, aborted,
                       std::make_integer_sequence<int, IG_MAX_LEN>{});
         if (aborted)
             break;
         __syncthreads();
     }
-    // the unused rest of each warp's slot chunk becomes sentinels
-    if (a.emit && !aborted) {
-        const unsigned long long base = g_slot_base[tid >> 5];
-        const unsigned left = g_slot_left[tid >> 5];
-        for (unsigned k = tid & 31; k < left; k += 32) {
-            const unsigned long long idx = base + k;
-            if (idx < a.rec_cap)
-                *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(kNoRow, 0u, 0u, 0u);
+    if (a.emit && !aborted)
+        fill_slot_tails(a);
+}
+
+// ---- nibble lanes (editDist <= 4): two rows per thread, 128 threads per band ----
+constexpr int kNibThreads = kBandRows / 2;
+
+// Hit flags of band_nib2 (bit 8c+7) -> bit c of a 4-column mask.
+__device__ __forceinline__ uint32_t nib_hits(uint32_t h)
+{
+    return ((h >> 7) & 1u) | ((h >> 14) & 2u) | ((h >> 21) & 4u) | ((h >> 28) & 8u);
+}
+
+// Records of one row's hits m (bit c: column col0 + c) at warp record numbers
+// j, j+1, ... of the slots sl.
+__device__ __forceinline__ void write_hits(const PairArgs &a, uint32_t m, const RowCtx &r, int32_t col0,
+                                           uint32_t &rank, const Slots &sl, unsigned &j)
+{
+    while (m) {
+        const int c = __ffs(m) - 1;
+        m &= m - 1u;
+        const unsigned long long idx = j < sl.n0 ? sl.b0 + j : sl.b1 + (j - sl.n0);
+        if (idx < a.rec_cap)
+            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(r.grow, r.base + (uint32_t)(col0 + c), rank, r.cell);
+        ++rank;
+        ++j;
+    }
+}
+
+// emit_mask for the two rows of a thread (at most 8 hits per unit).
+__device__ __forceinline__ void emit_two_rows(const PairArgs &a, uint32_t ma, uint32_t mb, const RowCtx &ra,
+                                              const RowCtx &rb, int32_t col0, uint32_t &rank_a, uint32_t &rank_b,
+                                              int lane)
+{
+    const uint32_t na = __popc(ma), nb = __popc(mb);
+    if (!a.emit) {
+        rank_a += na;
+        rank_b += nb;
+        return;
+    }
+    const uint32_t cnt = na + nb;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned total = 0, pre = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const unsigned bal = __ballot_sync(kFull, (cnt >> b) & 1u);
+        total += (unsigned)__popc(bal) << b;
+        pre += (unsigned)__popc(bal & lt) << b;
+    }
+    if (total == 0u)
+        return;
+    const Slots sl = take_slots(a, total, lane);
+    unsigned j = pre;
+    write_hits(a, ma, ra, col0, rank_a, sl, j);
+    write_hits(a, mb, rb, col0, rank_b, sl, j);
+}
+
+template <int L, bool CHECK>
+__device__ __forceinline__ void tile_pass_nib(const PairArgs &a, const uint4 *tile, int nu, int32_t c0,
+                                              const RowCtx &ra, const RowCtx &rb, const uint32_t (&W2)[L],
+                                              const BandConst &q, uint32_t &rank_a, uint32_t &rank_b, int lane)
+{
+    using BU = BandUnit<kModeNib>;
+    for (int u = 0; u < nu; ++u) {
+        const uint4 *src = tile + u * BU::kVec;
+        uint32_t sel[16];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            if (4 * v < L) {
+                const uint4 t4 = src[v];
+                sel[4 * v] = t4.x;
+                sel[4 * v + 1] = t4.y;
+                sel[4 * v + 2] = t4.z;
+                sel[4 * v + 3] = t4.w;
+            } else {
+                sel[4 * v] = sel[4 * v + 1] = sel[4 * v + 2] = sel[4 * v + 3] = 0u;
+            }
+        }
+        uint32_t he, ho;
+        myers::band_nib2<L>(W2, sel, q, he, ho);
+        if (__any_sync(kFull, (he | ho) != 0u)) {
+            const int32_t col0 = c0 + u * BU::kCols;
+            uint32_t ma = nib_hits(he), mb = nib_hits(ho);
+            if (CHECK) {
+                ma &= upper_mask<BU::kCols>(ra, col0);
+                mb &= upper_mask<BU::kCols>(rb, col0);
+            }
+            if (!CHECK || __any_sync(kFull, (ma | mb) != 0u))
+                emit_two_rows(a, ma, mb, ra, rb, col0, rank_a, rank_b, lane);
         }
     }
+}
+
+// One (band, segment) item of a nibble-lane job: thread t tests rows 2t and
+// 2t+1 of the band against the segment's columns, staged like run_item.
+template <int L>
+__device__ __forceinline__ void run_item_nib(const PairArgs &a, const JobDesc &J, int band, int seg,
+                                             uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
+                                             bool &aborted)
+{
+    using BU = BandUnit<kModeNib>;
+    constexpr int kTile = BU::kTileCols;
+    static_assert(kTile / BU::kCols * BU::kVec <= kSlotVec, "a tile must fit one staging slot");
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int32_t row0 = band * kBandRows;
+    RowCtx ra, rb;
+    ra.row = row0 + 2 * tid;
+    rb.row = ra.row + 1;
+    ra.ok = ra.row < J.n;
+    rb.ok = rb.row < J.n;
+    ra.n = rb.n = J.n;
+    ra.lim = rb.lim = J.lim;
+    ra.base = rb.base = (uint32_t)J.word_off;
+    ra.grow = (uint32_t)(J.word_off + ra.row);
+    rb.grow = ra.grow + 1u;
+    ra.cell = (uint32_t)(J.count_off + (long long)seg * J.n + ra.row);
+    rb.cell = ra.cell + 1u;
+    uint32_t W2[L];
+    {
+        uint32_t WB[L];
+        myers::band_windows<L, kModeNib>(a.words[J.word_off + (ra.ok ? ra.row : 0)], J.w, W2);
+        myers::band_windows<L, kModeNib>(a.words[J.word_off + (rb.ok ? rb.row : 0)], J.w, WB);
+#pragma unroll
+        for (int j = 0; j < L; ++j)
+            W2[j] |= WB[j] << 4;
+    }
+    BandConst q;
+    q.vp0 = J.vp0;
+    q.bm = J.bm;
+    q.c = J.cmask;
+    q.k = J.kthr;
+    q.one = a.one;
+    q.h16 = a.hi;
+    q.h28 = a.h28;
+    q.h31 = a.h31;
+    const int32_t c_lo = (int32_t)max((long long)seg << J.seg_shift, (long long)row0);
+    const int32_t c_hi = (int32_t)min((long long)(seg + 1) << J.seg_shift, (long long)J.n);
+    const long long row_end = (long long)row0 + kBandRows;
+    const bool check = ((long long)c_lo < row_end) || (row_end > (long long)J.n) || (c_hi % BU::kCols) != 0;
+    const int ntiles = (c_hi - c_lo + kTile - 1) / kTile;
+    const uint4 *units = a.units + J.unit_off;
+    uint32_t rank_a = 0, rank_b = 0;
+
+    if (tid == 0) {
+        for (int t = 0; t < 2 && t < ntiles; ++t) {
+            const int32_t c0 = c_lo + t * kTile;
+            const int nu = (min(kTile, c_hi - c0) + BU::kCols - 1) / BU::kCols;
+            const uint32_t bytes = (uint32_t)nu * BU::kBytes;
+            mbar_arrive_expect_tx(&bar[t], bytes);
+            bulk_g2s(&tile[t][0], units + (size_t)(c0 / BU::kCols) * BU::kVec, bytes, &bar[t]);
+        }
+    }
+    for (int t = 0; t < ntiles; ++t) {
+        const int b = t & 1;
+        bool timed_out = false;
+        const long long t_start = clock64();
+        while (!mbar_try_wait(&bar[b], (parity >> b) & 1u)) {
+            if (clock64() - t_start > kMaxWaitCycles) {
+                timed_out = true;
+                break;
+            }
+        }
+        parity ^= 1u << b;
+        if (__syncthreads_or(timed_out)) {
+            if (tid == 0)
+                atomicExch(a.status, kStatusTimeout);
+            aborted = true;
+            return;
+        }
+        const int32_t c0 = c_lo + t * kTile;
+        const int nu = (min(kTile, c_hi - c0) + BU::kCols - 1) / BU::kCols;
+        if (check)
+            tile_pass_nib<L, true>(a, tile[b], nu, c0, ra, rb, W2, q, rank_a, rank_b, lane);
+        else
+            tile_pass_nib<L, false>(a, tile[b], nu, c0, ra, rb, W2, q, rank_a, rank_b, lane);
+        __syncthreads();
+        if (tid == 0 && t + 2 < ntiles) {
+            const int32_t cn = c_lo + (t + 2) * kTile;
+            const int nun = (min(kTile, c_hi - cn) + BU::kCols - 1) / BU::kCols;
+            const uint32_t bytes = (uint32_t)nun * BU::kBytes;
+            mbar_arrive_expect_tx(&bar[b], bytes);
+            bulk_g2s(&tile[b][0], units + (size_t)(cn / BU::kCols) * BU::kVec, bytes, &bar[b]);
+        }
+    }
+    if (ra.ok)
+        a.counts[ra.cell] = rank_a;
+    if (rb.ok)
+        a.counts[rb.cell] = rank_b;
+    const unsigned hits = __reduce_add_sync(kFull, (ra.ok ? rank_a : 0u) + (rb.ok ? rank_b : 0u));
+    if (lane == 0 && hits != 0u)
+        atomicAdd(a.hit_count, (unsigned long long)hits);
+}
+
+template <int... Ls>
+__device__ __forceinline__ void dispatch_nib(int L, const PairArgs &a, const JobDesc &J, int band, int seg,
+                                             uint4 (*tile)[kSlotVec], uint64_t *bar, uint32_t &parity,
+                                             bool &aborted, std::integer_sequence<int, Ls...>)
+{
+    ((L == Ls + 1 ? run_item_nib<Ls + 1>(a, J, band, seg, tile, bar, parity, aborted) : void()), ...);
+}
+
+__global__ void __launch_bounds__(kNibThreads, 12) pair_kernel_nib(PairArgs a)
+{
+    __shared__ __align__(128) uint4 tile[2][kSlotVec];
+    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ long long item_sh;
+    item_loop(a, bar, item_sh, [&](const JobDesc J, int band, int seg, uint32_t &parity, bool &aborted) {
+        dispatch_nib(J.L, a, J, band, seg, tile, bar, parity, aborted, std::make_integer_sequence<int, IG_MAX_LEN>{});
+    });
 }
 
 // Per row: in-place exclusive prefix of its segment counts; degree -> out[row+1].
@@ -837,13 +1062,20 @@ int pair_grid(Ctx *ctx)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pair_kernel, kBandRows, 0);
         cudaGetLastError();
         ctx->pair_grid = std::max(bps, 1) * ctx->sm_count;
+        bps = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, pair_kernel_nib, kNibThreads, 0);
+        cudaGetLastError();
+        ctx->pair_grid_nib = std::max(bps, 1) * ctx->sm_count;
     }
     return ctx->pair_grid;
 }
 
 // Device-side layout of a batch.
 struct BatchLayout {
-    std::vector<JobDesc> desc;
+    std::vector<JobDesc> desc;      // every job, in batch order
+    std::vector<JobDesc> desc_nib;  // nibble-lane jobs with items, item_off over their own items
+    std::vector<JobDesc> desc_gen;  // the other jobs with items (pair_kernel)
+    long long items_nib = 0, items_gen = 0;
     long long items = 0;
     long long units = 0;       // column units over all jobs
     long long unit_vec = 0;    // uint4 of all unit streams
@@ -851,17 +1083,20 @@ struct BatchLayout {
     int64_t rows = 0;
 };
 
-bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
+// Each kernel (nibble lanes / the rest) gets about 24 items per CTA of its
+// grid, shared among its jobs in proportion to their pair tests.
+bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, BatchLayout &out)
 {
-    long double pairs_total = 0;
+    long double pairs_total[2] = {0, 0};
     for (const JobSpec &j : jobs)
-        pairs_total += (long double)j.n * (j.n > 0 ? j.n - 1 : 0) / 2;
-    const long long want_items = 24ll * grid;
+        pairs_total[myers::band_mode(j.len, j.min_ed) == kModeNib] += (long double)j.n * (j.n > 0 ? j.n - 1 : 0) / 2;
+    const long long want_items[2] = {24ll * grid_gen, 24ll * grid_nib};
     out = BatchLayout();
     for (const JobSpec &j : jobs) {
         JobDesc d{};
-        const long double share = pairs_total > 0 ? ((long double)j.n * (j.n - 1) / 2) / pairs_total : 0;
-        const PairPlan p = make_plan(j.n, std::max<long long>(1, (long long)(share * want_items)));
+        const int kn = myers::band_mode(j.len, j.min_ed) == kModeNib;
+        const long double share = pairs_total[kn] > 0 ? ((long double)j.n * (j.n - 1) / 2) / pairs_total[kn] : 0;
+        const PairPlan p = make_plan(j.n, std::max<long long>(1, (long long)(share * want_items[kn])));
         d.word_off = j.word_off;
         d.n = j.n;
         d.L = j.len;
@@ -881,7 +1116,7 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
             myers::band_constants(j.len, j.min_ed, d.mode, d.w, d.vp0, d.bm, d.cmask, d.kthr);
         long long units, vec;
         if (d.mode == kModeNib) {
-            units = ((long long)j.n + 7) / 8;
+            units = ((long long)j.n + 3) / 4;
             vec = 4;
         } else if (d.mode == kModeByte) {
             units = ((long long)j.n + 3) / 4;
@@ -904,6 +1139,13 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid, BatchLayout &out)
         out.counts += (long long)d.nseg * j.n;
         out.rows = std::max<int64_t>(out.rows, j.word_off + j.n);
         out.desc.push_back(d);
+        if (active && p.items > 0) {  // the kernel of its lane form takes its items
+            JobDesc k = d;
+            long long &space = d.mode == kModeNib ? out.items_nib : out.items_gen;
+            k.item_off = space;
+            space += p.items;
+            (d.mode == kModeNib ? out.desc_nib : out.desc_gen).push_back(k);
+        }
     }
     return out.counts < (1ll << 32);
 }
@@ -921,13 +1163,22 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
         return s;
     if ((s = ensure(ctx, ctx->counts, (size_t)B.counts * sizeof(uint32_t), "segment counts")) != IG_OK)
         return s;
-    if ((s = ensure(ctx, ctx->flags, 4 * sizeof(unsigned long long), "flags")) != IG_OK)
+    if ((s = ensure(ctx, ctx->flags, 8 * sizeof(unsigned long long), "flags")) != IG_OK)
         return s;
+    // job buffer: all jobs | job-boundary offsets (compaction) | nibble-kernel jobs | pair_kernel jobs
     const size_t jbytes = B.desc.size() * sizeof(JobDesc);
-    if ((s = ensure(ctx, ctx->jobs, jbytes + (B.desc.size() + 1) * sizeof(int64_t), "job table")) != IG_OK)
+    const size_t bbytes = (B.desc.size() + 1) * sizeof(int64_t);
+    const size_t nbytes = B.desc_nib.size() * sizeof(JobDesc), gbytes = B.desc_gen.size() * sizeof(JobDesc);
+    if ((s = ensure(ctx, ctx->jobs, jbytes + bbytes + nbytes + gbytes, "job table")) != IG_OK)
         return s;
-    IG_CUDA(cudaMemcpyAsync(ctx->jobs.ptr, B.desc.data(), jbytes, cudaMemcpyHostToDevice, st));
-    const JobDesc *d_jobs = static_cast<const JobDesc *>(ctx->jobs.ptr);
+    char *jbase = static_cast<char *>(ctx->jobs.ptr);
+    IG_CUDA(cudaMemcpyAsync(jbase, B.desc.data(), jbytes, cudaMemcpyHostToDevice, st));
+    if (nbytes)
+        IG_CUDA(cudaMemcpyAsync(jbase + jbytes + bbytes, B.desc_nib.data(), nbytes, cudaMemcpyHostToDevice, st));
+    if (gbytes)
+        IG_CUDA(cudaMemcpyAsync(jbase + jbytes + bbytes + nbytes, B.desc_gen.data(), gbytes, cudaMemcpyHostToDevice,
+                                st));
+    const JobDesc *d_jobs = reinterpret_cast<const JobDesc *>(jbase);
     const int njobs = (int)B.desc.size();
     phase_begin(ctx, IG_PHASE_PREP);
     if (B.units > 0)
@@ -937,19 +1188,15 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     ctx->launches++;
     IG_CUDA(cudaGetLastError());
     unsigned long long *flags = static_cast<unsigned long long *>(ctx->flags.ptr);
-    IG_CUDA(cudaMemsetAsync(flags, 0, 4 * sizeof(unsigned long long), st));
+    IG_CUDA(cudaMemsetAsync(flags, 0, 8 * sizeof(unsigned long long), st));
     PairArgs a;
     a.units = static_cast<const uint4 *>(ctx->sel.ptr);
     a.words = d_words;
-    a.jobs = d_jobs;
-    a.njobs = njobs;
-    a.items = B.items;
     a.one = 1u;
     a.two = 2u;
     a.hi = 1u << 16;
     a.h28 = 1u << 28;
     a.h31 = 1u << 31;
-    a.c16 = 16u;
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);
@@ -959,10 +1206,24 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
     a.emit = emit;
     phase_begin(ctx, IG_PHASE_PAIRS);
-    pair_kernel<<<grid, kBandRows, 0, st>>>(a);
+    if (B.items_gen > 0) {
+        a.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes + nbytes);
+        a.njobs = (int)B.desc_gen.size();
+        a.items = B.items_gen;
+        pair_kernel<<<grid, kBandRows, 0, st>>>(a);
+        ctx->launches++;
+        IG_CUDA(cudaGetLastError());
+    }
+    if (B.items_nib > 0) {
+        a.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes);
+        a.njobs = (int)B.desc_nib.size();
+        a.items = B.items_nib;
+        a.work = flags + 4;
+        pair_kernel_nib<<<ctx->pair_grid_nib, kNibThreads, 0, st>>>(a);
+        ctx->launches++;
+        IG_CUDA(cudaGetLastError());
+    }
     phase_end(ctx, IG_PHASE_PAIRS);
-    ctx->launches++;
-    IG_CUDA(cudaGetLastError());
     unsigned long long host_flags[4];
     IG_CUDA(cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, st));
     IG_CUDA(cudaStreamSynchronize(st));
@@ -1082,7 +1343,7 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         return s;
     const int grid = pair_grid(ctx);
     BatchLayout B;
-    if (!plan_batch(jobs, grid, B))
+    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, B))
         return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
     if (B.items == 0) {
         *edges = 0;
@@ -1104,7 +1365,7 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         return s;
     const int grid = pair_grid(ctx);
     BatchLayout B;
-    if (!plan_batch(jobs, grid, B))
+    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, B))
         return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
     const int32_t n = (int32_t)B.rows;
     g->ctx = ctx;
@@ -1135,7 +1396,8 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
             return set_error(ctx, IG_ERR_STATE, "record slots exceeded a buffer sized for them twice");
         // slots of a rerun differ from this pass only by the chunk tails of
         // the warps (scheduling), so leave room for all of them
-        const size_t tails = (size_t)grid * (kBandRows / 32) * kSlotChunk;
+        const size_t tails = ((size_t)grid * (kBandRows / 32) + (size_t)ctx->pair_grid_nib * (kNibThreads / 32)) *
+                             kSlotChunk;
         const size_t want = (size_t)(total + total / 8) + tails + 1024;
         s = ensure(ctx, ctx->records, want * sizeof(EdgeRecord), "edge records");
         if (s != IG_OK)

@@ -83,6 +83,7 @@ struct Ctx {
     DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs, aux;
     unsigned long long rec_capacity = 0;  // records that fit in `records`
     int pair_grid = 0;                    // persistent CTAs of the pair kernel
+    int pair_grid_nib = 0;                // ... of the nibble-lane pair kernel
     // optional per-phase timing (IG_PHASE_*)
     bool profiling = false;
     cudaEvent_t ev[6] = {};

@@ -189,32 +189,33 @@ __device__ __forceinline__ int myers_one_dist(uint32_t p01, uint32_t p23, const 
 // VN = 0.  The centre bit b = w is the main diagonal: D[L][L] = L - sum_j D0_j[w].
 // Many pair tests share one 32-bit word:
 //  * kNib  (w <= 1, min_ed <= 4): eight 4-bit lanes, band bits 0..2, bit 3 spare
+//    (two rows x four columns per thread)
 //  * kByte (w <= 3, min_ed <= 8): four 8-bit lanes, band bits 0..6, bit 7 spare
 // The spare bits of VP and Eq stay 0, so a lane's carry stops in its own spare
 // bit; D0 is masked to the band before it is shifted.  Y is not masked: its
 // spare bit may hold the next lane's bit 0, which reaches VN's spare bit only
 // (HP's spare bit is always 1, so VP's stays 0) and is masked out of D0.
-// Per character step kNib issues 10 ALU-pipe ops (2 PRMT + 8 LOP3) and 6
-// FMA-pipe ops (IMAD / IMAD.HI) for eight pair tests, kByte 9 ALU + 3.5 FMA
-// for four.  The match masks of all lanes come from PRMTs on a per-row window
-// register W_j whose byte c is the band window of Peq[c] at column j (kNib:
-// one PRMT on W_j for the even lanes' low nibbles, one on W_j * 16 for the
-// odd lanes' high nibbles).  Lane counters of the centre bits (weight 2^w
-// per byte) are compared with the threshold by adding 128 - 2^w (L - k) per
-// byte and reading bit 7.
+// Per character step kNib issues 9 ALU-pipe ops (1 PRMT + 8 LOP3) and 3
+// FMA-pipe ops (IMAD / IMAD.HI) for eight pair tests (two rows x four
+// columns), kByte 9 ALU + 3.5 FMA for four (one row x four columns).  The
+// match masks of all lanes come from one PRMT on a window register W_j whose
+// byte c is the band window of Peq[c] at column j (kNib: two rows' windows,
+// one per nibble).  Lane counters of the centre bits (weight 2^w per byte)
+// are compared with the threshold by adding 128 - 2^w (L - k) per byte and
+// reading bit 7.
 // ---------------------------------------------------------------------------
 enum LaneMode : int { kModeFull = 0, kModeNib = 1, kModeByte = 2 };
 
-// Column units of the banded modes.  kNib: 8 columns, one 32-bit word per
-// position (bits 0..15: chars of columns 0,2,4,6 as nibbles; bits 16..31:
-// columns 1,3,5,7).  kByte: 4 columns, 16 bits per position (nibble l = char
-// of column l), two positions per word.
+// Column units of the banded modes: 4 columns each.  kNib: one 32-bit word
+// per position (nibble l = char of column l in bits 0..15, bits 16..31 zero),
+// 16 words.  kByte: 16 bits per position (nibble l = char of column l), two
+// positions per word.
 template <int MODE>
 struct BandUnit {
-    static constexpr int kCols = MODE == kModeNib ? 8 : 4;
-    static constexpr int kVec = MODE == kModeNib ? 4 : 2;  // uint4 per unit
+    static constexpr int kCols = 4;                          // columns per unit
+    static constexpr int kVec = MODE == kModeNib ? 4 : 2;    // uint4 per unit
     static constexpr int kBytes = kVec * 16;
-    static constexpr int kTileCols = 1024;                  // columns per staged tile (8 KiB)
+    static constexpr int kTileCols = MODE == kModeNib ? 512 : 1024;  // columns per staged tile (8 KiB)
 };
 
 // Per-row band windows W_j, j = 0..L-1 (column j+1).
@@ -247,31 +248,29 @@ __device__ __forceinline__ void band_windows(uint32_t word, int w, uint32_t (&W)
 
 struct BandConst {
     uint32_t vp0, bm, c, k;       // initial VP, band mask, centre mask, threshold constant
-    uint32_t one, c16, h16, h28, h31;  // opaque 1, 16, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
+    uint32_t one, h16, h28, h31;  // opaque 1, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
 };
 
-// Eight pair tests (one row, eight columns); hit flags at bits 8m+7 of
-// he (column 2m) and ho (column 2m+1).
+// Eight pair tests: two rows A, B of one thread against four columns.  W2[j]
+// byte c holds row A's band window for character c in its low nibble and row
+// B's in its high nibble, so one PRMT with the column selector (nibble k =
+// character of column k at position j) yields all eight lanes: nibble 2k =
+// (A, column k), nibble 2k+1 = (B, column k).  Hit flags at bit 8k+7 of he
+// (row A) and ho (row B).
 template <int L>
-__device__ __forceinline__ void band_nib(const uint32_t (&W)[L], const uint32_t (&sel)[16], const BandConst &q,
-                                         uint32_t &he, uint32_t &ho)
+__device__ __forceinline__ void band_nib2(const uint32_t (&W2)[L], const uint32_t (&sel)[16], const BandConst &q,
+                                          uint32_t &he, uint32_t &ho)
 {
     uint32_t vp = q.vp0, vn = 0u, acc = 0u, be = 0u, bo = 0u;
 #pragma unroll
     for (int j = 0; j < L; ++j) {
-        const uint32_t s = sel[j];
-        const uint32_t e1 = __byte_perm(W[j], W[j], s);
-        const uint32_t whi = imad(W[j], q.c16, 0u);
-        const uint32_t e2 = __byte_perm(whi, whi, __umulhi(s, q.h16));
-        // e1 holds low nibbles only and e2 high nibbles only, so e1 | e2 is a
-        // sum, which the FMA pipe can form
-        const uint32_t eq = imad(e1, q.one, e2);
+        const uint32_t eq = __byte_perm(W2[j], W2[j], sel[j]);
         const uint32_t sum = imad(eq & vp, q.one, vp);
         const uint32_t d0 = ((sum ^ vp) | eq | vn) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
         acc = imad(d0 & q.c, q.one, acc);
-        if ((j + 1) % 7 == 0 || j == L - 1) {
+        if ((j + 1) % 7 == 0 || j == L - 1) {  // nibble counters hold at most 7 steps of 2^w
             be = imad(acc & 0x0f0f0f0fu, q.one, be);
             bo = imad(__umulhi(acc, q.h28) & 0x0f0f0f0fu, q.one, bo);
             acc = 0u;
