@@ -156,8 +156,15 @@ class BucketGreedy {
                 nt += v_[(size_t)j].deg >= 0;
             }
             todel_[(size_t)nt++] = x;
-            for (int32_t t = 0; t < nt; ++t)
+            // the neighbour lists of the ball's vertices are read next: fetch
+            // their heads a few vertices ahead
+            for (int32_t t = 0; t < nt && t < 4; ++t)
+                __builtin_prefetch(adj_ + ap_[todel_[(size_t)t]]);
+            for (int32_t t = 0; t < nt; ++t) {
+                if (t + 4 < nt)
+                    __builtin_prefetch(adj_ + ap_[todel_[(size_t)t + 4]]);
                 del_row_col(todel_[(size_t)t]);
+            }
         }
         return cnt;
     }
@@ -189,8 +196,8 @@ class BucketGreedy {
     }
 
     // Neighbours are visited in blocks of 8: their degrees are loaded together
-    // (independent loads overlap) and only the live ones (degree > 0) are
-    // walked through a bitmask.  Exact: within one pass over m[i] the
+    // (independent loads overlap, the next block's are prefetched) and only
+    // the live ones (degree > 0) are walked through a bitmask.  Exact: within one pass over m[i] the
     // neighbours are distinct and decrease_sum(j) changes only deg[j].
     void del_row_col(int32_t i)
     {
@@ -200,6 +207,8 @@ class BucketGreedy {
         const int64_t e = ap_[i + 1];
         for (int64_t k = ap_[i]; k < e; k += 8) {
             const int m = (int)std::min<int64_t>(8, e - k);
+            for (int64_t q = k + 8; q < std::min<int64_t>(k + 16, e); ++q)  // next block's degrees
+                __builtin_prefetch(&v_[(size_t)(adj_[q] - base_)]);
             int32_t jj[8], dd[8];
             unsigned live = 0;
             for (int t = 0; t < m; ++t) {
