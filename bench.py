@@ -275,6 +275,14 @@ def run_batch_section(ctx, reps: int = 3) -> dict:
         t0 = time.perf_counter()
         books, edges = solve_batch(jobs, host_threads=cores, ctx=ctx)
         t_batch.append(time.perf_counter() - t0)
+    # the same batch with direct launches instead of the captured CUDA graphs
+    ctx.set_graphs(False)
+    t_direct = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        solve_batch(jobs, host_threads=cores, ctx=ctx)
+        t_direct.append(time.perf_counter() - t0)
+    ctx.set_graphs(True)
     # one more pass with per-phase events (they add syncs, so it is not timed)
     ctx.set_profiling(True)
     solve_batch(jobs, host_threads=cores, ctx=ctx)
@@ -292,6 +300,8 @@ def run_batch_section(ctx, reps: int = 3) -> dict:
             "jobs": len(jobs), "pair_tests": pairs, "edges": int(np.sum(edges)),
             "codebook_words": int(sum(len(b) for b in books)),
             "batched_jobs_per_s": len(jobs) / tb, "batched_s": tb,
+            "batched_direct_launches_jobs_per_s": len(jobs) / min(t_direct),
+            "work_split_items_per_cta": ctx.work_split(1)[0], "work_split_tuned": ctx.work_split(1)[1],
             "plain_jobs_per_s": len(jobs) / t_plain, "plain_s": t_plain,
             "speedup_vs_plain": t_plain / tb,
             "batched_pair_kernel_gpairs_per_s": (pairs / (pair_ms / 1e3) / 1e9) if pair_ms else None,
@@ -474,7 +484,7 @@ def run_ours(args, wl, rank, world, dist):
 
     import torch
 
-    from indexgen_b200 import Context, build_conflict_graph
+    from indexgen_b200 import Context, build_conflict_graph, lane_form
     from indexgen_b200._lib import check, lib
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
@@ -597,6 +607,10 @@ def run_ours(args, wl, rank, world, dist):
                        "frac": (comp_bytes / comp_avg_s / 1e9 / hbm_peak) if comp_launches else None,
                        "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs"},
         "gpu_launches": launches,
+        "work_split": {"lane_form": ["full", "nibble", "byte"][lane_form(L, d)],
+                       "items_per_cta": ctx.work_split(lane_form(L, d))[0],
+                       "tuned": ctx.work_split(lane_form(L, d))[1]},
+        "cuda_graphs": dict(zip(("launches", "instantiations", "updates"), ctx.graph_stats())),
         "clocks": clk,
         "greedy": {"ms": greedy_ms, "codebook": int(len(sel)), "order_threads": 1, "where": "host C++ (library)"},
     }

@@ -71,6 +71,54 @@ int64_t ig_ctx_launches(const ig_ctx *ctx);
 ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable);
 ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches);
 
+/* ---- work split and its autotuner -------------------------------------- */
+/* No counterpart in the reference, whose tiling is fixed: 16,384 x 16,384
+ * pair tiles, one launch each with 16 x 16-thread blocks
+ * (src/cuda_edit_distance.py:278, :335-338, :384-425).  The
+ * pair kernels are persistent: each CTA claims (256-row band x segment) item
+ * tiles of the pair triangle from a device counter.  The work split -- target
+ * items per CTA of the grid -- sets how many items a batch is cut into and so
+ * each job's segment width (256 .. 16,384 columns): wide tiles amortise the
+ * per-item setup, narrow ones even out the end of the launch.  It is kept per
+ * lane form of the pair kernel, which (len, min_ed) selects: */
+#define IG_LANES_FULL 0   /* full Myers lanes (min_ed > 8)                   */
+#define IG_LANES_NIBBLE 1 /* 8 banded nibble lanes per word (min_ed <= 4)    */
+#define IG_LANES_BYTE 2   /* 4 banded byte lanes per word (5 <= min_ed <= 8) */
+/* Lane form for (len, min_ed); -1 when len is out of range. */
+int ig_lane_form(int len, int min_ed);
+/* Times the count-only pair pass of a representative job (host or device
+ * words, as ig_graph_build) for each candidate split whose plan differs
+ * (6, 12, 24, 48, 96 items per CTA; CUDA events on the context's stream,
+ * best of two after a warm-up) and keeps the fastest for the job's lane
+ * form; *items_per_cta (optional) = the choice.  Results never depend on
+ * the split.  With autotuning on (the default) a context tunes each lane
+ * form by itself on the first build that is worth it: on the build's jobs
+ * of that form, or on a 131,072-word sample of the largest of them when
+ * they hold more than 2^33 pair tests. */
+ig_status ig_ctx_autotune(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
+                          int32_t *items_per_cta);
+/* Pins a lane form's split (1..4096 items per CTA; the untuned default is
+ * 24); the automatic tuner then leaves that form alone. */
+ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_cta);
+/* The current split of a lane form and whether it was tuned or pinned. */
+ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned);
+/* Automatic tuning on (1, default) or off (0). */
+ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable);
+
+/* ---- CUDA graphs of the batch pipeline ---------------------------------- */
+/* Each build (single job or batch) runs as two CUDA graph launches on the
+ * context's stream: the pair pass (job table upload, selector streams, the
+ * persistent pair kernel(s), status readback) and the compaction (row
+ * offsets, scan, scatter into CSR, job bounds), with one host wait after
+ * each (the edge count sizes the CSR; the bounds split it into jobs).  Each
+ * pass is captured and applied to the context's cached executable graph with
+ * cudaGraphExecUpdate, so a new batch of a known shape costs no
+ * instantiation.  On by default; per-phase timing (ig_ctx_set_profiling)
+ * runs the same calls without graphs.  Results never depend on it. */
+ig_status ig_ctx_set_graphs(ig_ctx *ctx, int enable);
+/* Graph launches, instantiations and in-place updates on this context. */
+ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *instantiations, int64_t *updates);
+
 /* ---- host-side input preparation (no device work) ---------------------- */
 
 /* '0'..'3' text rows, `stride` bytes apart, to packed words.  Replaces the

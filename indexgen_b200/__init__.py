@@ -10,6 +10,9 @@ from .graph import (  # noqa: F401
     ConflictGraph,
     Context,
     IndexGenError,
+    LANES_BYTE,
+    LANES_FULL,
+    LANES_NIBBLE,
     Server,
     apply_filters,
     assign_centers,
@@ -21,6 +24,7 @@ from .graph import (  # noqa: F401
     count_conflicts,
     default_context,
     fill_adj_list_gpu,
+    lane_form,
     pack_sequences,
     random_cluster_fit,
     read_adj_list,

@@ -24,6 +24,8 @@ EXPORTS = (
     "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_codebooks", "ig_solve_batch",
     "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
     "ig_server_stats", "ig_server_destroy",
+    "ig_lane_form", "ig_ctx_autotune", "ig_ctx_set_work_split", "ig_ctx_work_split", "ig_ctx_set_autotune",
+    "ig_ctx_set_graphs", "ig_ctx_graph_stats",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -99,6 +101,13 @@ def _declare(L):
         "ig_server_cancel": (_int, [_vp, _i64]),
         "ig_server_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
         "ig_server_destroy": (_int, [_vp]),
+        "ig_lane_form": (_int, [_int, _int]),
+        "ig_ctx_autotune": (_int, [_vp, _vp, _i32, _int, _int, _int, ctypes.POINTER(_i32)]),
+        "ig_ctx_set_work_split": (_int, [_vp, _int, _i32]),
+        "ig_ctx_work_split": (_int, [_vp, _int, ctypes.POINTER(_i32), ctypes.POINTER(_int)]),
+        "ig_ctx_set_autotune": (_int, [_vp, _int]),
+        "ig_ctx_set_graphs": (_int, [_vp, _int]),
+        "ig_ctx_graph_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

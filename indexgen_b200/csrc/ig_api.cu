@@ -376,6 +376,11 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
         for (cudaEvent_t e : ctx->ev)
             if (e)
                 cudaEventDestroy(e);
+        for (cudaGraphExec_t x : ctx->graph_exec)
+            if (x)
+                cudaGraphExecDestroy(x);
+        if (ctx->stage)
+            cudaFreeHost(ctx->stage);
         cudaGetLastError();
     }
     delete ctx;
@@ -823,6 +828,87 @@ ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int 
     if (s != IG_OK)
         return s;
     return ig::count_batch(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, edges);
+}
+
+int ig_lane_form(int len, int min_ed)
+{
+    if (len < 1 || len > IG_MAX_LEN)
+        return -1;
+    return ig::lane_form(len, min_ed);
+}
+
+ig_status ig_ctx_autotune(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
+                          int32_t *items_per_cta)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    if (ig::check_job(words, n, len) != IG_OK || n < 2 || min_ed < 1)
+        return ig::set_error(ctx, IG_ERR_INPUT, "autotune needs n >= 2 words of 1 <= len <= 16 and min_ed >= 1");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    const uint32_t *d_words = nullptr;
+    ig_status s = ig::stage_words(ctx, words, n, words_on_device, &d_words);
+    int chosen = 0;
+    if (s == IG_OK)
+        s = ig::autotune(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, &chosen);
+    if (s == IG_OK && items_per_cta)
+        *items_per_cta = chosen;
+    return s;
+}
+
+ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_cta)
+{
+    if (!ctx || lane_form < 0 || lane_form > 2 || items_per_cta < 1 || items_per_cta > 4096)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->items_per_cta[lane_form] = items_per_cta;
+    ctx->tuned[lane_form] = true;
+    return IG_OK;
+}
+
+ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned)
+{
+    if (!ctx || lane_form < 0 || lane_form > 2)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (items_per_cta)
+        *items_per_cta = ctx->items_per_cta[lane_form];
+    if (tuned)
+        *tuned = ctx->tuned[lane_form] ? 1 : 0;
+    return IG_OK;
+}
+
+ig_status ig_ctx_set_graphs(ig_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->use_graphs = enable != 0;
+    return IG_OK;
+}
+
+ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *instantiations, int64_t *updates)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    if (launches)
+        *launches = ctx->graph_launches;
+    if (instantiations)
+        *instantiations = ctx->graph_instantiations;
+    if (updates)
+        *updates = ctx->graph_updates;
+    return IG_OK;
+}
+
+ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable)
+{
+    if (!ctx)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->autotune = enable != 0;
+    return IG_OK;
 }
 
 }  // extern "C"

@@ -27,6 +27,7 @@
 // bit-exact by construction (no sort, no dependence on scheduling).
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 
 #include "ig_internal.h"
 #include "ig_myers.cuh"
@@ -1055,6 +1056,84 @@ ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
             return cuda_error(ctx, e_, #call);                                                                 \
     } while (0)
 
+// Page-locked staging of at least `bytes` (the context stream must be idle:
+// a graph in flight may still read the old block).
+ig_status ensure_stage(Ctx *ctx, size_t bytes)
+{
+    if (ctx->stage && ctx->stage_bytes >= bytes)
+        return IG_OK;
+    const size_t want = std::max<size_t>({bytes, ctx->stage_bytes + ctx->stage_bytes / 2, 4096});
+    if (ctx->stage) {
+        cudaFreeHost(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_bytes = 0;
+    }
+    cudaError_t e = cudaHostAlloc(&ctx->stage, want, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        ctx->stage = nullptr;
+        return set_error(ctx, IG_ERR_OOM, "page-locked staging allocation failed");
+    }
+    ctx->stage_bytes = want;
+    return IG_OK;
+}
+
+// Queues the work of `enqueue` (a callable that queues onto ctx->stream and
+// returns the first CUDA error) as one CUDA graph launch: the calls are
+// captured, the capture is applied to the context's cached executable graph
+// `slot` by cudaGraphExecUpdate when the topology is unchanged (only kernel
+// arguments, grids and copy addresses differ between batches) or
+// instantiated afresh, and the executable graph is launched on the stream.
+// With graphs off, or with per-phase event timing on (events recorded inside
+// a capture are not timed), the calls run directly on the stream.
+template <class F>
+ig_status run_graph(Ctx *ctx, int slot, const char *what, F &&enqueue)
+{
+    cudaStream_t st = ctx->stream;
+    if (!ctx->use_graphs || ctx->profiling) {
+        const cudaError_t e = enqueue();
+        return e == cudaSuccess ? IG_OK : cuda_error(ctx, e, what);
+    }
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, what);
+    const cudaError_t qe = enqueue();
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(st, &graph);
+    if (qe != cudaSuccess || e != cudaSuccess) {
+        if (graph)
+            cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return cuda_error(ctx, qe != cudaSuccess ? qe : e, what);
+    }
+    cudaGraphExec_t &exec = ctx->graph_exec[slot];
+    if (exec) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(exec, graph, &info) == cudaSuccess) {
+            ctx->graph_updates++;
+        } else {
+            cudaGetLastError();
+            cudaGraphExecDestroy(exec);
+            exec = nullptr;
+        }
+    }
+    if (!exec) {
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        if (e != cudaSuccess) {
+            exec = nullptr;
+            cudaGraphDestroy(graph);
+            return cuda_error(ctx, e, what);
+        }
+        ctx->graph_instantiations++;
+    }
+    cudaGraphDestroy(graph);
+    e = cudaGraphLaunch(exec, st);
+    if (e != cudaSuccess)
+        return cuda_error(ctx, e, what);
+    ctx->graph_launches++;
+    return IG_OK;
+}
+
 int pair_grid(Ctx *ctx)
 {
     if (ctx->pair_grid == 0) {
@@ -1083,20 +1162,24 @@ struct BatchLayout {
     int64_t rows = 0;
 };
 
-// Each kernel (nibble lanes / the rest) gets about 24 items per CTA of its
-// grid, shared among its jobs in proportion to their pair tests.
-bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, BatchLayout &out)
+// Each kernel (nibble lanes / the rest) gets items_per_cta[lane form] items
+// per CTA of its grid (the work split, 24 unless the autotuner chose
+// another), shared among its jobs in proportion to their pair tests.
+bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, const int (&items_per_cta)[3],
+                BatchLayout &out)
 {
     long double pairs_total[2] = {0, 0};
     for (const JobSpec &j : jobs)
         pairs_total[myers::band_mode(j.len, j.min_ed) == kModeNib] += (long double)j.n * (j.n > 0 ? j.n - 1 : 0) / 2;
-    const long long want_items[2] = {24ll * grid_gen, 24ll * grid_nib};
+    const long long grids[2] = {grid_gen, grid_nib};
     out = BatchLayout();
     for (const JobSpec &j : jobs) {
         JobDesc d{};
-        const int kn = myers::band_mode(j.len, j.min_ed) == kModeNib;
+        const int lane_form = myers::band_mode(j.len, j.min_ed);
+        const int kn = lane_form == kModeNib;
         const long double share = pairs_total[kn] > 0 ? ((long double)j.n * (j.n - 1) / 2) / pairs_total[kn] : 0;
-        const PairPlan p = make_plan(j.n, std::max<long long>(1, (long long)(share * want_items[kn])));
+        const long long want = (long long)items_per_cta[lane_form] * grids[kn];
+        const PairPlan p = make_plan(j.n, std::max<long long>(1, (long long)(share * want)));
         d.word_off = j.word_off;
         d.n = j.n;
         d.L = j.len;
@@ -1169,26 +1252,25 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     const size_t jbytes = B.desc.size() * sizeof(JobDesc);
     const size_t bbytes = (B.desc.size() + 1) * sizeof(int64_t);
     const size_t nbytes = B.desc_nib.size() * sizeof(JobDesc), gbytes = B.desc_gen.size() * sizeof(JobDesc);
-    if ((s = ensure(ctx, ctx->jobs, jbytes + bbytes + nbytes + gbytes, "job table")) != IG_OK)
+    const size_t table = jbytes + bbytes + nbytes + gbytes;
+    if ((s = ensure(ctx, ctx->jobs, table, "job table")) != IG_OK)
         return s;
-    char *jbase = static_cast<char *>(ctx->jobs.ptr);
-    IG_CUDA(cudaMemcpyAsync(jbase, B.desc.data(), jbytes, cudaMemcpyHostToDevice, st));
+    // staging: the job table image | 8 flag words read back | job bounds read back
+    const size_t flag_off = (table + 63) & ~size_t(63), bound_off = flag_off + 64;
+    if ((s = ensure_stage(ctx, bound_off + bbytes)) != IG_OK)
+        return s;
+    char *stage = static_cast<char *>(ctx->stage);
+    std::memcpy(stage, B.desc.data(), jbytes);
+    std::memset(stage + jbytes, 0, bbytes);
     if (nbytes)
-        IG_CUDA(cudaMemcpyAsync(jbase + jbytes + bbytes, B.desc_nib.data(), nbytes, cudaMemcpyHostToDevice, st));
+        std::memcpy(stage + jbytes + bbytes, B.desc_nib.data(), nbytes);
     if (gbytes)
-        IG_CUDA(cudaMemcpyAsync(jbase + jbytes + bbytes + nbytes, B.desc_gen.data(), gbytes, cudaMemcpyHostToDevice,
-                                st));
+        std::memcpy(stage + jbytes + bbytes + nbytes, B.desc_gen.data(), gbytes);
+    unsigned long long *host_flags = reinterpret_cast<unsigned long long *>(stage + flag_off);
+    char *jbase = static_cast<char *>(ctx->jobs.ptr);
     const JobDesc *d_jobs = reinterpret_cast<const JobDesc *>(jbase);
     const int njobs = (int)B.desc.size();
-    phase_begin(ctx, IG_PHASE_PREP);
-    if (B.units > 0)
-        prep_units<<<(unsigned)((B.units + 255) / 256), 256, 0, st>>>(d_words, d_jobs, njobs, B.units,
-                                                                       static_cast<uint4 *>(ctx->sel.ptr));
-    phase_end(ctx, IG_PHASE_PREP);
-    ctx->launches++;
-    IG_CUDA(cudaGetLastError());
     unsigned long long *flags = static_cast<unsigned long long *>(ctx->flags.ptr);
-    IG_CUDA(cudaMemsetAsync(flags, 0, 8 * sizeof(unsigned long long), st));
     PairArgs a;
     a.units = static_cast<const uint4 *>(ctx->sel.ptr);
     a.words = d_words;
@@ -1205,27 +1287,50 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.rec_cap = emit ? ctx->rec_capacity : 0;
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
     a.emit = emit;
-    phase_begin(ctx, IG_PHASE_PAIRS);
-    if (B.items_gen > 0) {
-        a.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes + nbytes);
-        a.njobs = (int)B.desc_gen.size();
-        a.items = B.items_gen;
-        pair_kernel<<<grid, kBandRows, 0, st>>>(a);
-        ctx->launches++;
-        IG_CUDA(cudaGetLastError());
-    }
-    if (B.items_nib > 0) {
-        a.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes);
-        a.njobs = (int)B.desc_nib.size();
-        a.items = B.items_nib;
-        a.work = flags + 4;
-        pair_kernel_nib<<<ctx->pair_grid_nib, kNibThreads, 0, st>>>(a);
-        ctx->launches++;
-        IG_CUDA(cudaGetLastError());
-    }
-    phase_end(ctx, IG_PHASE_PAIRS);
-    unsigned long long host_flags[4];
-    IG_CUDA(cudaMemcpyAsync(host_flags, flags, sizeof(host_flags), cudaMemcpyDeviceToHost, st));
+    const int grid_nib = ctx->pair_grid_nib;
+    int64_t launched = 0;
+    s = run_graph(ctx, 0, "pair pass", [&]() -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(jbase, stage, table, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess)
+            return e;
+        phase_begin(ctx, IG_PHASE_PREP);
+        if (B.units > 0) {
+            prep_units<<<(unsigned)((B.units + 255) / 256), 256, 0, st>>>(d_words, d_jobs, njobs, B.units,
+                                                                           static_cast<uint4 *>(ctx->sel.ptr));
+            launched++;
+        }
+        phase_end(ctx, IG_PHASE_PREP);
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+        if ((e = cudaMemsetAsync(flags, 0, 8 * sizeof(unsigned long long), st)) != cudaSuccess)
+            return e;
+        phase_begin(ctx, IG_PHASE_PAIRS);
+        PairArgs k = a;
+        if (B.items_gen > 0) {
+            k.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes + nbytes);
+            k.njobs = (int)B.desc_gen.size();
+            k.items = B.items_gen;
+            pair_kernel<<<grid, kBandRows, 0, st>>>(k);
+            launched++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+        }
+        if (B.items_nib > 0) {
+            k.jobs = reinterpret_cast<const JobDesc *>(jbase + jbytes + bbytes);
+            k.njobs = (int)B.desc_nib.size();
+            k.items = B.items_nib;
+            k.work = flags + 4;
+            pair_kernel_nib<<<grid_nib, kNibThreads, 0, st>>>(k);
+            launched++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+        }
+        phase_end(ctx, IG_PHASE_PAIRS);
+        return cudaMemcpyAsync(host_flags, flags, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    });
+    ctx->launches += launched;
+    if (s != IG_OK)
+        return s;
     IG_CUDA(cudaStreamSynchronize(st));
     phase_collect(ctx);
     if (static_cast<int>(host_flags[2] & 0xffffffffu) == kStatusTimeout)
@@ -1343,7 +1448,7 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         return s;
     const int grid = pair_grid(ctx);
     BatchLayout B;
-    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, B))
+    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, ctx->items_per_cta, B))
         return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
     if (B.items == 0) {
         *edges = 0;
@@ -1357,15 +1462,137 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     return IG_OK;
 }
 
-ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, Graph *g)
+// Work-split autotuner.  The pair kernels walk (256-row band x segment) item
+// tiles; items_per_cta sets how many a batch is cut into, and so the segment
+// width (256 .. 16,384 columns) of each job's item tiles: wide tiles amortise
+// the per-item row setup and tile staging, narrow ones even out the end of the
+// persistent launch.  The tuner times the count-only pair pass of `jobs` (all
+// of one lane form) with CUDA events on the context's stream for each
+// candidate whose plan differs from the ones already timed (best of two runs
+// after one warm-up) and keeps the fastest for that lane form.
+ig_status autotune(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int *chosen)
 {
-    cudaStream_t st = ctx->stream;
+    static const int kCandidates[] = {6, 12, 24, 48, 96};
+    if (jobs.empty())
+        return set_error(ctx, IG_ERR_INPUT, "autotune needs a job");
+    const int mode = myers::band_mode(jobs[0].len, jobs[0].min_ed);
+    for (const JobSpec &j : jobs)
+        if (myers::band_mode(j.len, j.min_ed) != mode)
+            return set_error(ctx, IG_ERR_INPUT, "autotune jobs must share one lane form");
     ig_status s = check_jobs(ctx, jobs);
     if (s != IG_OK)
         return s;
     const int grid = pair_grid(ctx);
+    const int before = ctx->items_per_cta[mode];
+    // distinct plans only: candidates that cut the jobs identically are one
+    std::vector<int> cands;
+    std::vector<std::vector<int>> shifts;
+    for (int c : kCandidates) {
+        int tune[3] = {ctx->items_per_cta[0], ctx->items_per_cta[1], ctx->items_per_cta[2]};
+        tune[mode] = c;
+        BatchLayout B;
+        if (!plan_batch(jobs, grid, ctx->pair_grid_nib, tune, B))
+            return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
+        std::vector<int> sh;
+        for (const JobDesc &d : B.desc)
+            sh.push_back(d.seg_shift);
+        if (std::find(shifts.begin(), shifts.end(), sh) == shifts.end()) {
+            shifts.push_back(sh);
+            cands.push_back(c);
+        }
+    }
+    int best = before;
+    if (cands.size() > 1) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            if (e0)
+                cudaEventDestroy(e0);
+            return cuda_error(ctx, cudaGetLastError(), "autotune events");
+        }
+        float best_ms = 1e30f;
+        int64_t edges = 0;
+        for (size_t k = 0; k < cands.size() && s == IG_OK; ++k) {
+            ctx->items_per_cta[mode] = cands[k];
+            if (k == 0)
+                s = count_batch(ctx, d_words, jobs, &edges);  // warm-up: workspaces grow here
+            float ms = 1e30f;
+            for (int rep = 0; rep < 2 && s == IG_OK; ++rep) {
+                cudaEventRecord(e0, ctx->stream);
+                s = count_batch(ctx, d_words, jobs, &edges);
+                cudaEventRecord(e1, ctx->stream);
+                const cudaError_t e = cudaEventSynchronize(e1);
+                float t = 0.f;
+                if (e != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+                    s = cuda_error(ctx, e != cudaSuccess ? e : cudaGetLastError(), "autotune timing");
+                ms = std::min(ms, t);
+            }
+            if (s == IG_OK && ms < best_ms) {
+                best_ms = ms;
+                best = cands[k];
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    } else if (!cands.empty()) {
+        best = before;  // every candidate gives the same plan: nothing to choose
+    }
+    ctx->items_per_cta[mode] = s == IG_OK ? best : before;
+    if (s == IG_OK && cands.size() > 1) {
+        ctx->tuned[mode] = true;
+        ctx->tune_runs++;
+    }
+    if (chosen)
+        *chosen = ctx->items_per_cta[mode];
+    return s;
+}
+
+int lane_form(int len, int min_ed) { return myers::band_mode(len, min_ed); }
+
+ig_status autotune_jobs(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs)
+{
+    if (!ctx->autotune)
+        return IG_OK;
+    for (int mode = 0; mode < 3; ++mode) {
+        if (ctx->tuned[mode])
+            continue;
+        std::vector<JobSpec> sub;
+        long double pairs = 0;
+        size_t largest = 0;
+        for (const JobSpec &j : jobs)
+            if (j.n > 1 && j.min_ed > 0 && myers::band_mode(j.len, j.min_ed) == mode) {
+                sub.push_back(j);
+                pairs += (long double)j.n * (j.n - 1) / 2;
+                if (j.n > sub[largest].n)
+                    largest = sub.size() - 1;
+            }
+        if (sub.empty())
+            continue;
+        // Time the real jobs when a pass is short (<= 2^33 pair tests, about
+        // 10 ms on nibble lanes); otherwise the first 131,072 words of the
+        // largest job stand in for them.
+        if (pairs > (long double)(1ull << 33)) {
+            JobSpec one = sub[largest];
+            one.n = std::min<int32_t>(one.n, 131072);
+            sub.assign(1, one);
+        }
+        ig_status s = autotune(ctx, d_words, sub, nullptr);
+        if (s != IG_OK)
+            return s;
+    }
+    return IG_OK;
+}
+
+ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, Graph *g)
+{
+    cudaStream_t st = ctx->stream;
+    ig_status s = check_jobs(ctx, jobs);
+    if (s == IG_OK)
+        s = autotune_jobs(ctx, d_words, jobs);
+    if (s != IG_OK)
+        return s;
+    const int grid = pair_grid(ctx);
     BatchLayout B;
-    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, B))
+    if (!plan_batch(jobs, grid, ctx->pair_grid_nib, ctx->items_per_cta, B))
         return set_error(ctx, IG_ERR_CAPACITY, "batch too large for one launch");
     const int32_t n = (int32_t)B.rows;
     g->ctx = ctx;
@@ -1406,35 +1633,55 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     }
     g->edges = (int64_t)total;
     IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
-    IG_CUDA(cudaMemsetAsync(g->d_row_ptr, 0, sizeof(int64_t), st));
     const JobDesc *d_jobs = static_cast<const JobDesc *>(ctx->jobs.ptr);
     const int njobs = (int)B.desc.size();
-    phase_begin(ctx, IG_PHASE_COMPACT);
-    row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr), d_jobs, njobs,
-                                                               n, g->d_row_ptr);
-    ctx->launches++;
-    IG_CUDA(cudaGetLastError());
-    // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
-    s = inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1);
-    if (s != IG_OK)
-        return s;
-    if (total > 0) {
-        const int sgrid =
-            (int)std::min<unsigned long long>((slots + 255) / 256, (unsigned long long)ctx->sm_count * 16);
-        scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), slots,
-                                                g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
-                                                g->d_cols);
-        ctx->launches++;
-        IG_CUDA(cudaGetLastError());
-    }
-    phase_end(ctx, IG_PHASE_COMPACT);
     int64_t *d_bounds = reinterpret_cast<int64_t *>(static_cast<char *>(ctx->jobs.ptr) + B.desc.size() * sizeof(JobDesc));
-    job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, d_jobs, njobs, n, d_bounds);
-    ctx->launches++;
-    IG_CUDA(cudaGetLastError());
-    IG_CUDA(cudaMemcpyAsync(g->job_edge_off.data(), d_bounds, (njobs + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost,
-                            st));
+    // the scan workspace is sized before the capture (no allocation inside it)
+    if ((s = ensure(ctx, ctx->scan_tmp, (size_t)((int64_t)n + kScanChunk) / kScanChunk * sizeof(int64_t),
+                    "scan workspace")) != IG_OK)
+        return s;
+    // job bounds come back through the staging block, after the flag words
+    const size_t table = B.desc.size() * sizeof(JobDesc) + (B.desc.size() + 1) * sizeof(int64_t) +
+                         (B.desc_nib.size() + B.desc_gen.size()) * sizeof(JobDesc);
+    int64_t *host_bounds = reinterpret_cast<int64_t *>(static_cast<char *>(ctx->stage) +
+                                                       ((table + 63) & ~size_t(63)) + 64);
+    const int64_t launches_before = ctx->launches;
+    s = run_graph(ctx, 1, "compaction", [&]() -> cudaError_t {
+        cudaError_t e = cudaMemsetAsync(g->d_row_ptr, 0, sizeof(int64_t), st);
+        if (e != cudaSuccess)
+            return e;
+        phase_begin(ctx, IG_PHASE_COMPACT);
+        row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr), d_jobs,
+                                                                   njobs, n, g->d_row_ptr);
+        ctx->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+        // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
+        if (inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1) != IG_OK)
+            return cudaErrorUnknown;
+        if (total > 0) {
+            const int sgrid =
+                (int)std::min<unsigned long long>((slots + 255) / 256, (unsigned long long)ctx->sm_count * 16);
+            scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), slots,
+                                                    g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
+                                                    g->d_cols);
+            ctx->launches++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+        }
+        phase_end(ctx, IG_PHASE_COMPACT);
+        job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, d_jobs, njobs, n, d_bounds);
+        ctx->launches++;
+        if ((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+        return cudaMemcpyAsync(host_bounds, d_bounds, (njobs + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    });
+    if (s != IG_OK) {
+        ctx->launches = launches_before;
+        return s;
+    }
     IG_CUDA(cudaStreamSynchronize(st));
+    std::memcpy(g->job_edge_off.data(), host_bounds, (njobs + 1) * sizeof(int64_t));
     phase_collect(ctx);
     if (g->job_edge_off[(size_t)njobs] != (int64_t)total)
         return set_error(ctx, IG_ERR_STATE, "row offsets disagree with the edge count");

@@ -84,6 +84,12 @@ struct Ctx {
     unsigned long long rec_capacity = 0;  // records that fit in `records`
     int pair_grid = 0;                    // persistent CTAs of the pair kernel
     int pair_grid_nib = 0;                // ... of the nibble-lane pair kernel
+    // work split per lane form (full Myers, nibble, byte lanes): target items
+    // per CTA, chosen by the autotuner (ig_ctx_autotune) or left at 24
+    int items_per_cta[3] = {24, 24, 24};
+    bool tuned[3] = {false, false, false};
+    bool autotune = true;  // tune a lane form on its first batch worth tuning
+    int64_t tune_runs = 0; // tuner runs that chose among several plans
     // optional per-phase timing (IG_PHASE_*)
     bool profiling = false;
     cudaEvent_t ev[6] = {};
@@ -91,6 +97,17 @@ struct Ctx {
     int64_t phase_launches[3] = {0, 0, 0};
     bool phase_pending[3] = {false, false, false};
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
+    // CUDA graphs of the batch pipeline: [0] the pair pass (job table upload,
+    // selector streams, pair kernels, status readback), [1] the compaction
+    // (row offsets, scan, scatter, job bounds).  Each build captures the pass
+    // and applies it to the cached executable graph with cudaGraphExecUpdate
+    // (a new instantiation only when the topology changed).
+    bool use_graphs = true;
+    cudaGraphExec_t graph_exec[2] = {};
+    int64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
+    // page-locked staging of the graphs' host copies
+    void *stage = nullptr;
+    size_t stage_bytes = 0;
 };
 
 // Records an event pair around a phase when profiling is on.
@@ -131,6 +148,16 @@ PairPlan make_plan(int32_t n, long long target_items);
 // Device pipeline stages (ig_graph.cu).  Jobs index into d_words.
 ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, Graph *g);
 ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int64_t *edges);
+// Lane form of the pair kernel for (len, min_ed): kModeFull 0, kModeNib 1,
+// kModeByte 2 (ig_graph.cu).
+int lane_form(int len, int min_ed);
+// Times the work-split candidates on `jobs` (one lane form) and keeps the
+// fastest for that lane form (ig_graph.cu).
+ig_status autotune(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int *chosen);
+// With ctx->autotune set, tunes every lane form of `jobs` not tuned yet on
+// this context (on the jobs themselves, or on a 131,072-word sample of the
+// largest when they hold more than 2^33 pair tests).  Caller holds ctx->mu.
+ig_status autotune_jobs(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs);
 
 // In-place inclusive scan of m int64 on the context stream (ig_graph.cu).
 ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m);

@@ -64,6 +64,47 @@ class Context:
     def reserve(self, edges: int):
         check(lib().ig_ctx_reserve(self.handle, int(edges)), "ig_ctx_reserve", self.handle)
 
+    def autotune(self, words, L: int, min_ed: int) -> int:
+        """Time the work-split candidates on this job (host words, or a
+        device tensor on this context's GPU) and keep the fastest for its lane
+        form; returns the chosen items per CTA (ig_ctx_autotune)."""
+        got = ctypes.c_int32()
+        if hasattr(words, "data_ptr") and getattr(words, "is_cuda", False):
+            wptr, n, on_dev = ctypes.c_void_p(words.data_ptr()), int(words.numel()), 1
+        else:
+            w = _words_array(words)
+            wptr, n, on_dev = ptr(w), len(w), 0
+        check(lib().ig_ctx_autotune(self.handle, wptr, n, int(L), int(min_ed), on_dev, ctypes.byref(got)),
+              "ig_ctx_autotune", self.handle)
+        return int(got.value)
+
+    def set_work_split(self, lane_form: int, items_per_cta: int):
+        """Pin a lane form's split (IG_LANES_FULL=0, NIBBLE=1, BYTE=2)."""
+        check(lib().ig_ctx_set_work_split(self.handle, int(lane_form), int(items_per_cta)),
+              "ig_ctx_set_work_split", self.handle)
+
+    def work_split(self, lane_form: int):
+        """(items per CTA, tuned-or-pinned) of a lane form."""
+        v = ctypes.c_int32()
+        t = ctypes.c_int()
+        check(lib().ig_ctx_work_split(self.handle, int(lane_form), ctypes.byref(v), ctypes.byref(t)),
+              "ig_ctx_work_split", self.handle)
+        return int(v.value), bool(t.value)
+
+    def set_graphs(self, enable: bool):
+        """Run builds as captured CUDA graphs (default) or as direct launches."""
+        check(lib().ig_ctx_set_graphs(self.handle, int(bool(enable))), "ig_ctx_set_graphs", self.handle)
+
+    def graph_stats(self):
+        """(graph launches, instantiations, in-place updates) so far."""
+        v = [ctypes.c_int64() for _ in range(3)]
+        check(lib().ig_ctx_graph_stats(self.handle, *[ctypes.byref(x) for x in v]), "ig_ctx_graph_stats",
+              self.handle)
+        return tuple(int(x.value) for x in v)
+
+    def set_autotune(self, enable: bool):
+        check(lib().ig_ctx_set_autotune(self.handle, int(bool(enable))), "ig_ctx_set_autotune", self.handle)
+
     def close(self):
         if self.handle:
             lib().ig_ctx_destroy(self.handle)
@@ -206,6 +247,14 @@ class ConflictGraph:
             self.close()
         except Exception:
             pass
+
+
+LANES_FULL, LANES_NIBBLE, LANES_BYTE = 0, 1, 2
+
+
+def lane_form(L: int, min_ed: int) -> int:
+    """Lane form of the pair kernel for (L, min_ed) (ig_lane_form)."""
+    return int(lib().ig_lane_form(int(L), int(min_ed)))
 
 
 def build_conflict_graph(words, L: int, min_ed: int, ctx: Context | None = None) -> ConflictGraph:
