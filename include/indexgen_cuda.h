@@ -106,15 +106,15 @@ ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, 
 ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable);
 
 /* ---- CUDA graphs of the batch pipeline ---------------------------------- */
-/* Each build (single job or batch) runs as two CUDA graph launches on the
- * context's stream: the pair pass (job table upload, selector streams, the
- * persistent pair kernel(s), status readback) and the compaction (row
- * offsets, scan, scatter into CSR, job bounds), with one host wait after
- * each (the edge count sizes the CSR; the bounds split it into jobs).  Each
- * pass is captured and applied to the context's cached executable graph with
- * cudaGraphExecUpdate, so a new batch of a known shape costs no
- * instantiation.  On by default; per-phase timing (ig_ctx_set_profiling)
- * runs the same calls without graphs.  Results never depend on it. */
+/* Each build (single job or batch) is one CUDA graph launch on the
+ * context's stream -- job table upload, selector streams, the persistent pair
+ * kernel(s), then the compaction into CSR (row offsets, scan, scatter, job
+ * bounds) and the status readback -- with one host wait at the end.  A build
+ * whose arguments equal the cached graph's relaunches it; otherwise the calls
+ * are captured and applied to the cached executable graph with
+ * cudaGraphExecUpdate, so a batch of a known shape costs no instantiation.
+ * On by default; per-phase timing (ig_ctx_set_profiling) runs the same calls
+ * without graphs.  Results never depend on it. */
 ig_status ig_ctx_set_graphs(ig_ctx *ctx, int enable);
 /* Graph launches, instantiations and in-place updates on this context. */
 ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *instantiations, int64_t *updates);

@@ -225,6 +225,8 @@ struct PairArgs {
     uint32_t hi;
     uint32_t h28;
     uint32_t h31;
+    uint32_t gather;  // 0x00204081 and 16, opaque: hit flags -> column mask on the FMA pipe
+    uint32_t h4;
     unsigned long long *work;
     unsigned long long *rec_count;  // record slots handed out (chunks of kSlotChunk)
     unsigned long long *hit_count;  // pair tests that are edges (exact)
@@ -283,6 +285,39 @@ __device__ __forceinline__ Slots take_slots(const PairArgs &a, unsigned total, i
     return s;
 }
 
+// Hit flags at bits 7, 15, 23, 31 of h (all other bits clear) -> bits 0..3.
+// The multiply by 2^21 + 2^14 + 2^7 + 1 moves bit 8c+7 to bit 28+c and puts
+// every other partial product on a distinct bit below 28 or above 31 (no
+// carries), and the high half of a multiply by 16 is bits 28..31: two FMA-pipe
+// operations instead of seven shifts and masks on the ALU pipe.
+__device__ __forceinline__ uint32_t hit_columns(uint32_t h, const PairArgs &a)
+{
+    return __umulhi(myers::imad(h, a.gather, 0u), a.h4);
+}
+
+// Warp total of cnt and this lane's exclusive prefix.  When no lane has more
+// than one hit (the usual case on sparse graphs) one ballot gives both;
+// otherwise the bit planes of cnt (kPlanes of them) are balloted.
+template <int kPlanes>
+__device__ __forceinline__ void warp_count_prefix(uint32_t cnt, int lane, unsigned &total, unsigned &pre)
+{
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned some = __ballot_sync(kFull, cnt != 0u);
+    if (__all_sync(kFull, cnt <= 1u)) {
+        total = (unsigned)__popc(some);
+        pre = (unsigned)__popc(some & lt);
+        return;
+    }
+    total = 0;
+    pre = 0;
+#pragma unroll
+    for (int b = 0; b < kPlanes; ++b) {
+        const unsigned bal = __ballot_sync(kFull, (cnt >> b) & 1u);
+        total += (unsigned)__popc(bal) << b;
+        pre += (unsigned)__popc(bal & lt) << b;
+    }
+}
+
 // Everything one thread needs about its row while it walks a segment.
 struct RowCtx {
     int32_t row;     // job-local row
@@ -319,16 +354,10 @@ __device__ __forceinline__ void emit_mask(const PairArgs &a, uint32_t m, const R
         rank += cnt;
         return;
     }
-    // warp total and this lane's exclusive prefix from the bit planes of cnt
+    // warp total and this lane's exclusive prefix
     constexpr int kPlanes = NC >= 8 ? 4 : (NC >= 4 ? 3 : (NC >= 2 ? 2 : 1));
-    const unsigned lt = (1u << lane) - 1u;
-    unsigned total = 0, pre = 0;
-#pragma unroll
-    for (int b = 0; b < kPlanes; ++b) {
-        const unsigned bal = __ballot_sync(kFull, (cnt >> b) & 1u);
-        total += (unsigned)__popc(bal) << b;
-        pre += (unsigned)__popc(bal & lt) << b;
-    }
+    unsigned total, pre;
+    warp_count_prefix<kPlanes>(cnt, lane, total, pre);
     if (total == 0u)
         return;
     const Slots sl = take_slots(a, total, lane);
@@ -422,7 +451,7 @@ __device__ __forceinline__ void tile_pass_band(const PairArgs &a, const uint4 *t
         if (__any_sync(kFull, he != 0u)) {
             const int32_t base_col = c0 + u * BU::kCols;
             // hit flag of column q at bit 8q+7
-            uint32_t m = ((he >> 7) & 1u) | ((he >> 14) & 2u) | ((he >> 21) & 4u) | ((he >> 28) & 8u);
+            uint32_t m = hit_columns(he, a);
             if (CHECK)
                 m &= upper_mask<BU::kCols>(r, base_col);
             if (!CHECK || __any_sync(kFull, m != 0u))
@@ -682,12 +711,6 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
 // ---- nibble lanes (editDist <= 4): two rows per thread, 128 threads per band ----
 constexpr int kNibThreads = kBandRows / 2;
 
-// Hit flags of band_nib2 (bit 8c+7) -> bit c of a 4-column mask.
-__device__ __forceinline__ uint32_t nib_hits(uint32_t h)
-{
-    return ((h >> 7) & 1u) | ((h >> 14) & 2u) | ((h >> 21) & 4u) | ((h >> 28) & 8u);
-}
-
 // Records of one row's hits m (bit c: column col0 + c) at warp record numbers
 // j, j+1, ... of the slots sl.
 __device__ __forceinline__ void write_hits(const PairArgs &a, uint32_t m, const RowCtx &r, int32_t col0,
@@ -715,15 +738,8 @@ __device__ __forceinline__ void emit_two_rows(const PairArgs &a, uint32_t ma, ui
         rank_b += nb;
         return;
     }
-    const uint32_t cnt = na + nb;
-    const unsigned lt = (1u << lane) - 1u;
-    unsigned total = 0, pre = 0;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const unsigned bal = __ballot_sync(kFull, (cnt >> b) & 1u);
-        total += (unsigned)__popc(bal) << b;
-        pre += (unsigned)__popc(bal & lt) << b;
-    }
+    unsigned total, pre;
+    warp_count_prefix<4>(na + nb, lane, total, pre);
     if (total == 0u)
         return;
     const Slots sl = take_slots(a, total, lane);
@@ -757,7 +773,7 @@ __device__ __forceinline__ void tile_pass_nib(const PairArgs &a, const uint4 *ti
         myers::band_nib2<L>(W2, sel, q, he, ho);
         if (__any_sync(kFull, (he | ho) != 0u)) {
             const int32_t col0 = c0 + u * BU::kCols;
-            uint32_t ma = nib_hits(he), mb = nib_hits(ho);
+            uint32_t ma = hit_columns(he, a), mb = hit_columns(ho, a);
             if (CHECK) {
                 ma &= upper_mask<BU::kCols>(ra, col0);
                 mb &= upper_mask<BU::kCols>(rb, col0);
@@ -1005,10 +1021,16 @@ __global__ void scan_add(int64_t *__restrict__ x, int64_t m, const int64_t *__re
             x[base + k] += add;
 }
 
-__global__ void scatter_records(const EdgeRecord *__restrict__ rec, unsigned long long nrec,
-                                const int64_t *__restrict__ row_ptr, const uint32_t *__restrict__ counts,
-                                int32_t *__restrict__ cols)
+// The slot count comes from the pair pass's counter on the device (the
+// scatter is queued in the same graph, before the host has seen it); a pass
+// whose slots overflowed the record buffer is rerun, so it scatters nothing.
+__global__ void scatter_records(const EdgeRecord *__restrict__ rec, const unsigned long long *__restrict__ d_slots,
+                                unsigned long long cap, const int64_t *__restrict__ row_ptr,
+                                const uint32_t *__restrict__ counts, int32_t *__restrict__ cols)
 {
+    const unsigned long long nrec = *d_slots;
+    if (nrec > cap)
+        return;
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < nrec;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const uint4 r = *reinterpret_cast<const uint4 *>(rec + i);
@@ -1086,14 +1108,27 @@ ig_status ensure_stage(Ctx *ctx, size_t bytes)
 // instantiated afresh, and the executable graph is launched on the stream.
 // With graphs off, or with per-phase event timing on (events recorded inside
 // a capture are not timed), the calls run directly on the stream.
+//
+// `sig` lists every pointer, size, grid and scalar argument the calls bake
+// into the graph (not the contents of the staging block, which the graph's
+// copy reads when it runs); when it equals the one of the cached graph, the
+// cached graph is launched as it is, without a capture.
 template <class F>
-ig_status run_graph(Ctx *ctx, int slot, const char *what, F &&enqueue)
+ig_status run_graph(Ctx *ctx, int slot, const std::vector<uint64_t> &sig, const char *what, F &&enqueue)
 {
     cudaStream_t st = ctx->stream;
     if (!ctx->use_graphs || ctx->profiling) {
         const cudaError_t e = enqueue();
         return e == cudaSuccess ? IG_OK : cuda_error(ctx, e, what);
     }
+    if (ctx->graph_exec[slot] && ctx->graph_sig[slot] == sig) {
+        const cudaError_t e = cudaGraphLaunch(ctx->graph_exec[slot], st);
+        if (e != cudaSuccess)
+            return cuda_error(ctx, e, what);
+        ctx->graph_launches++;
+        return IG_OK;
+    }
+    ctx->graph_sig[slot].clear();
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess)
         return cuda_error(ctx, e, what);
@@ -1127,6 +1162,7 @@ ig_status run_graph(Ctx *ctx, int slot, const char *what, F &&enqueue)
         ctx->graph_instantiations++;
     }
     cudaGraphDestroy(graph);
+    ctx->graph_sig[slot] = sig;
     e = cudaGraphLaunch(exec, st);
     if (e != cudaSuccess)
         return cuda_error(ctx, e, what);
@@ -1157,6 +1193,7 @@ struct BatchLayout {
     long long items_nib = 0, items_gen = 0;
     long long items = 0;
     long long units = 0;       // column units over all jobs
+    long long pairs = 0;       // pair tests over the jobs with items (bounds the edges)
     long long unit_vec = 0;    // uint4 of all unit streams
     long long counts = 0;      // per-(segment, row) cells
     int64_t rows = 0;
@@ -1217,6 +1254,7 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, co
         if (!active)
             d.nseg = 0;
         out.items += active ? p.items : 0;
+        out.pairs += active ? (long long)j.n * (j.n - 1) / 2 : 0;
         out.units += units;
         out.unit_vec += units * vec;
         out.counts += (long long)d.nseg * j.n;
@@ -1233,12 +1271,23 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, co
     return out.counts < (1ll << 32);
 }
 
-// Runs prep + the pair kernel for a planned batch.  On return *total holds
-// the number of edges; records are complete iff *total <= capacity.
-// One pair pass.  *slots = record slots handed out (>= *hits; the records
-// buffer must hold them all for the pass to be complete), *hits = edges.
-ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int grid, int emit,
-                    unsigned long long *slots, unsigned long long *hits)
+// Compaction of a build pass: the CSR it fills.
+struct CompactOut {
+    int64_t *row_ptr = nullptr;  // n + 1
+    int32_t *cols = nullptr;     // room for min(record capacity, pair tests) columns
+    int32_t n = 0;
+};
+
+// One pass over a planned batch: job table upload, selector streams, the pair
+// kernel(s) and, for a build (`out` set), the compaction into out's CSR (row
+// offsets from the per-(row, segment) counts, scan, scatter of the records,
+// job bounds) -- queued as ONE graph launch with one host wait at the end.
+// *slots = record slots handed out (>= *hits; the pass is complete iff they
+// fit the record buffer -- otherwise its CSR is void and the caller grows the
+// buffer and reruns), *hits = edges; bounds (build only) = row_ptr at the
+// job boundaries.
+ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int grid, const CompactOut *out,
+                   unsigned long long *slots, unsigned long long *hits, int64_t *bounds)
 {
     cudaStream_t st = ctx->stream;
     ig_status s;
@@ -1248,6 +1297,11 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
         return s;
     if ((s = ensure(ctx, ctx->flags, 8 * sizeof(unsigned long long), "flags")) != IG_OK)
         return s;
+    // the scan workspace is sized here: nothing allocates inside a capture
+    const int64_t m = out ? (int64_t)out->n + 1 : 0;
+    if (out && (s = ensure(ctx, ctx->scan_tmp, (size_t)((m + kScanChunk - 1) / kScanChunk) * sizeof(int64_t),
+                           "scan workspace")) != IG_OK)
+        return s;
     // job buffer: all jobs | job-boundary offsets (compaction) | nibble-kernel jobs | pair_kernel jobs
     const size_t jbytes = B.desc.size() * sizeof(JobDesc);
     const size_t bbytes = (B.desc.size() + 1) * sizeof(int64_t);
@@ -1255,7 +1309,7 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     const size_t table = jbytes + bbytes + nbytes + gbytes;
     if ((s = ensure(ctx, ctx->jobs, table, "job table")) != IG_OK)
         return s;
-    // staging: the job table image | 8 flag words read back | job bounds read back
+    // staging: the job table image | 4 flag words read back | job bounds read back
     const size_t flag_off = (table + 63) & ~size_t(63), bound_off = flag_off + 64;
     if ((s = ensure_stage(ctx, bound_off + bbytes)) != IG_OK)
         return s;
@@ -1267,8 +1321,10 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     if (gbytes)
         std::memcpy(stage + jbytes + bbytes + nbytes, B.desc_gen.data(), gbytes);
     unsigned long long *host_flags = reinterpret_cast<unsigned long long *>(stage + flag_off);
+    int64_t *host_bounds = reinterpret_cast<int64_t *>(stage + bound_off);
     char *jbase = static_cast<char *>(ctx->jobs.ptr);
     const JobDesc *d_jobs = reinterpret_cast<const JobDesc *>(jbase);
+    int64_t *d_bounds = reinterpret_cast<int64_t *>(jbase + jbytes);
     const int njobs = (int)B.desc.size();
     unsigned long long *flags = static_cast<unsigned long long *>(ctx->flags.ptr);
     PairArgs a;
@@ -1279,24 +1335,39 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
     a.hi = 1u << 16;
     a.h28 = 1u << 28;
     a.h31 = 1u << 31;
+    a.gather = 0x00204081u;
+    a.h4 = 16u;
     a.work = flags + 0;
     a.rec_count = flags + 1;
     a.status = reinterpret_cast<int *>(flags + 2);
     a.hit_count = flags + 3;
     a.rec = static_cast<EdgeRecord *>(ctx->records.ptr);
-    a.rec_cap = emit ? ctx->rec_capacity : 0;
+    a.rec_cap = out ? ctx->rec_capacity : 0;
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
-    a.emit = emit;
+    a.emit = out ? 1 : 0;
     const int grid_nib = ctx->pair_grid_nib;
+    const unsigned prep_grid = (unsigned)((B.units + 255) / 256);
+    const int n = out ? out->n : 0;
+    // scatter grid: enough threads for the slots the pass can hand out
+    const unsigned long long cap = ctx->rec_capacity;
+    const int sgrid = (int)std::min<unsigned long long>((std::min<unsigned long long>(cap, (unsigned long long)B.pairs) + 255) / 256 + 1,
+                                                        (unsigned long long)ctx->sm_count * 16);
+    const std::vector<uint64_t> sig = {
+        (uint64_t)(uintptr_t)stage,  table, (uint64_t)(uintptr_t)jbase, (uint64_t)(uintptr_t)d_words,
+        (uint64_t)B.units,           (uint64_t)njobs, (uint64_t)(uintptr_t)ctx->sel.ptr,
+        (uint64_t)(uintptr_t)flags,  (uint64_t)(uintptr_t)ctx->records.ptr, cap,
+        (uint64_t)(uintptr_t)ctx->counts.ptr, (uint64_t)a.emit, (uint64_t)B.items_gen, (uint64_t)B.items_nib,
+        B.desc_nib.size(),           B.desc_gen.size(), (uint64_t)grid, (uint64_t)grid_nib,
+        out ? (uint64_t)(uintptr_t)out->row_ptr : 0, out ? (uint64_t)(uintptr_t)out->cols : 0, (uint64_t)n,
+        (uint64_t)sgrid,             (uint64_t)(uintptr_t)ctx->scan_tmp.ptr};
     int64_t launched = 0;
-    s = run_graph(ctx, 0, "pair pass", [&]() -> cudaError_t {
+    s = run_graph(ctx, out ? 0 : 1, sig, out ? "build pass" : "count pass", [&]() -> cudaError_t {
         cudaError_t e = cudaMemcpyAsync(jbase, stage, table, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess)
             return e;
         phase_begin(ctx, IG_PHASE_PREP);
         if (B.units > 0) {
-            prep_units<<<(unsigned)((B.units + 255) / 256), 256, 0, st>>>(d_words, d_jobs, njobs, B.units,
-                                                                           static_cast<uint4 *>(ctx->sel.ptr));
+            prep_units<<<prep_grid, 256, 0, st>>>(d_words, d_jobs, njobs, B.units, static_cast<uint4 *>(ctx->sel.ptr));
             launched++;
         }
         phase_end(ctx, IG_PHASE_PREP);
@@ -1326,6 +1397,33 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
                 return e;
         }
         phase_end(ctx, IG_PHASE_PAIRS);
+        if (out) {
+            if ((e = cudaMemsetAsync(out->row_ptr, 0, sizeof(int64_t), st)) != cudaSuccess)
+                return e;
+            phase_begin(ctx, IG_PHASE_COMPACT);
+            row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr),
+                                                                       d_jobs, njobs, n, out->row_ptr);
+            launched++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+            // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
+            if (inclusive_scan_i64(ctx, out->row_ptr, m) != IG_OK)
+                return cudaErrorLaunchFailure;
+            scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), flags + 1, cap,
+                                                    out->row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
+                                                    out->cols);
+            launched++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+            phase_end(ctx, IG_PHASE_COMPACT);
+            job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(out->row_ptr, d_jobs, njobs, n,
+                                                                             d_bounds);
+            launched++;
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                return e;
+            if ((e = cudaMemcpyAsync(host_bounds, d_bounds, bbytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+                return e;
+        }
         return cudaMemcpyAsync(host_flags, flags, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     });
     ctx->launches += launched;
@@ -1337,6 +1435,8 @@ ig_status run_pairs(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int
         return set_error(ctx, IG_ERR_TIMEOUT, "pair kernel: staged tile never arrived (bounded wait expired)");
     *slots = host_flags[1];
     *hits = host_flags[3];
+    if (bounds)
+        std::memcpy(bounds, host_bounds, bbytes);
     return IG_OK;
 }
 
@@ -1455,7 +1555,7 @@ ig_status count_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         return IG_OK;
     }
     unsigned long long slots = 0, hits = 0;
-    s = run_pairs(ctx, d_words, B, grid, 0, &slots, &hits);
+    s = run_pass(ctx, d_words, B, grid, nullptr, &slots, &hits, nullptr);
     if (s != IG_OK)
         return s;
     *edges = (int64_t)hits;
@@ -1614,11 +1714,22 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     }
     unsigned long long slots = 0, total = 0;
     for (int attempt = 0;; ++attempt) {
-        s = run_pairs(ctx, d_words, B, grid, 1, &slots, &total);
+        // columns: room for every record slot the pass may fill (at most one
+        // per pair test), so the compaction runs in the same graph as the
+        // pair kernels, before the host has seen the edge count
+        const size_t col_cap = (size_t)std::min<unsigned long long>(ctx->rec_capacity, (unsigned long long)B.pairs);
+        IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>(col_cap, 1) * sizeof(int32_t), st));
+        CompactOut out;
+        out.row_ptr = g->d_row_ptr;
+        out.cols = g->d_cols;
+        out.n = n;
+        s = run_pass(ctx, d_words, B, grid, &out, &slots, &total, g->job_edge_off.data());
         if (s != IG_OK)
             return s;
         if (slots <= ctx->rec_capacity)
             break;
+        cudaFreeAsync(g->d_cols, st);
+        g->d_cols = nullptr;
         if (attempt > 0)
             return set_error(ctx, IG_ERR_STATE, "record slots exceeded a buffer sized for them twice");
         // slots of a rerun differ from this pass only by the chunk tails of
@@ -1632,57 +1743,7 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
     }
     g->edges = (int64_t)total;
-    IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
-    const JobDesc *d_jobs = static_cast<const JobDesc *>(ctx->jobs.ptr);
     const int njobs = (int)B.desc.size();
-    int64_t *d_bounds = reinterpret_cast<int64_t *>(static_cast<char *>(ctx->jobs.ptr) + B.desc.size() * sizeof(JobDesc));
-    // the scan workspace is sized before the capture (no allocation inside it)
-    if ((s = ensure(ctx, ctx->scan_tmp, (size_t)((int64_t)n + kScanChunk) / kScanChunk * sizeof(int64_t),
-                    "scan workspace")) != IG_OK)
-        return s;
-    // job bounds come back through the staging block, after the flag words
-    const size_t table = B.desc.size() * sizeof(JobDesc) + (B.desc.size() + 1) * sizeof(int64_t) +
-                         (B.desc_nib.size() + B.desc_gen.size()) * sizeof(JobDesc);
-    int64_t *host_bounds = reinterpret_cast<int64_t *>(static_cast<char *>(ctx->stage) +
-                                                       ((table + 63) & ~size_t(63)) + 64);
-    const int64_t launches_before = ctx->launches;
-    s = run_graph(ctx, 1, "compaction", [&]() -> cudaError_t {
-        cudaError_t e = cudaMemsetAsync(g->d_row_ptr, 0, sizeof(int64_t), st);
-        if (e != cudaSuccess)
-            return e;
-        phase_begin(ctx, IG_PHASE_COMPACT);
-        row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr), d_jobs,
-                                                                   njobs, n, g->d_row_ptr);
-        ctx->launches++;
-        if ((e = cudaGetLastError()) != cudaSuccess)
-            return e;
-        // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
-        if (inclusive_scan_i64(ctx, g->d_row_ptr, (int64_t)n + 1) != IG_OK)
-            return cudaErrorUnknown;
-        if (total > 0) {
-            const int sgrid =
-                (int)std::min<unsigned long long>((slots + 255) / 256, (unsigned long long)ctx->sm_count * 16);
-            scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), slots,
-                                                    g->d_row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
-                                                    g->d_cols);
-            ctx->launches++;
-            if ((e = cudaGetLastError()) != cudaSuccess)
-                return e;
-        }
-        phase_end(ctx, IG_PHASE_COMPACT);
-        job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, d_jobs, njobs, n, d_bounds);
-        ctx->launches++;
-        if ((e = cudaGetLastError()) != cudaSuccess)
-            return e;
-        return cudaMemcpyAsync(host_bounds, d_bounds, (njobs + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-    });
-    if (s != IG_OK) {
-        ctx->launches = launches_before;
-        return s;
-    }
-    IG_CUDA(cudaStreamSynchronize(st));
-    std::memcpy(g->job_edge_off.data(), host_bounds, (njobs + 1) * sizeof(int64_t));
-    phase_collect(ctx);
     if (g->job_edge_off[(size_t)njobs] != (int64_t)total)
         return set_error(ctx, IG_ERR_STATE, "row offsets disagree with the edge count");
     return IG_OK;

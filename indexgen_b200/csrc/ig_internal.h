@@ -97,13 +97,15 @@ struct Ctx {
     int64_t phase_launches[3] = {0, 0, 0};
     bool phase_pending[3] = {false, false, false};
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
-    // CUDA graphs of the batch pipeline: [0] the pair pass (job table upload,
-    // selector streams, pair kernels, status readback), [1] the compaction
-    // (row offsets, scan, scatter, job bounds).  Each build captures the pass
-    // and applies it to the cached executable graph with cudaGraphExecUpdate
-    // (a new instantiation only when the topology changed).
+    // CUDA graphs of the batch pipeline: [0] a build pass (job table upload,
+    // selector streams, pair kernels, row offsets, scan, scatter into CSR,
+    // job bounds, readback), [1] a count-only pass.  A pass whose arguments
+    // equal the cached graph's relaunches it; otherwise it is captured and
+    // applied to the cached executable graph with cudaGraphExecUpdate (a new
+    // instantiation only when the topology changed).
     bool use_graphs = true;
     cudaGraphExec_t graph_exec[2] = {};
+    std::vector<uint64_t> graph_sig[2];  // arguments baked into each cached graph
     int64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
