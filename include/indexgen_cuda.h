@@ -92,9 +92,11 @@ int ig_lane_form(int len, int min_ed);
  * best of two after a warm-up) and keeps the fastest for the job's lane
  * form; *items_per_cta (optional) = the choice.  Results never depend on
  * the split.  With autotuning on (the default) a context tunes each lane
- * form by itself on the first build that is worth it: on the build's jobs
- * of that form, or on a 131,072-word sample of the largest of them when
- * they hold more than 2^33 pair tests. */
+ * form by itself on the first batch build (two or more jobs) whose
+ * candidates cut differently: on the batch's jobs of that form, or on a
+ * 131,072-word sample of the largest of them when they hold more than 2^33
+ * pair tests.  Single-job builds keep the current split (24 until tuned),
+ * so a process that builds once pays no timing passes. */
 ig_status ig_ctx_autotune(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
                           int32_t *items_per_cta);
 /* Pins a lane form's split (1..4096 items per CTA; the untuned default is

@@ -1650,7 +1650,10 @@ int lane_form(int len, int min_ed) { return myers::band_mode(len, min_ed); }
 
 ig_status autotune_jobs(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs)
 {
-    if (!ctx->autotune)
+    // Batches only: their uneven jobs are where the split matters, and a
+    // one-job build (often the only one of a process) would pay the timing
+    // passes up front; ig_ctx_autotune tunes for single jobs on request.
+    if (!ctx->autotune || jobs.size() < 2)
         return IG_OK;
     for (int mode = 0; mode < 3; ++mode) {
         if (ctx->tuned[mode])

@@ -156,9 +156,10 @@ int lane_form(int len, int min_ed);
 // Times the work-split candidates on `jobs` (one lane form) and keeps the
 // fastest for that lane form (ig_graph.cu).
 ig_status autotune(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs, int *chosen);
-// With ctx->autotune set, tunes every lane form of `jobs` not tuned yet on
-// this context (on the jobs themselves, or on a 131,072-word sample of the
-// largest when they hold more than 2^33 pair tests).  Caller holds ctx->mu.
+// With ctx->autotune set and a batch of two or more jobs, tunes every lane
+// form of `jobs` not tuned yet on this context (on the jobs themselves, or on
+// a 131,072-word sample of the largest when they hold more than 2^33 pair
+// tests).  Caller holds ctx->mu.
 ig_status autotune_jobs(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSpec> &jobs);
 
 // In-place inclusive scan of m int64 on the context stream (ig_graph.cu).

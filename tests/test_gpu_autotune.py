@@ -62,9 +62,10 @@ def test_autotune_picks_a_candidate_per_lane_form(L, d, form):
 
 
 def test_automatic_tuning_on_first_large_build(oracle):
-    """A fresh context tunes a lane form by itself on the first build whose
-    splits differ, and the graph equals the untuned build's."""
-    from indexgen_b200 import Context, LANES_BYTE, build_batch, workloads as W
+    """A fresh context tunes a lane form by itself on the first batch build
+    whose splits differ (not on a single-job build), and the graph equals the
+    untuned build's."""
+    from indexgen_b200 import Context, LANES_BYTE, build_batch, build_conflict_graph, workloads as W
 
     parts = [W.uniform_words(n, 13, 300 + n) for n in (70000, 20000, 5000)]
     jobs = [(p, 13, 6) for p in parts]
@@ -72,6 +73,10 @@ def test_automatic_tuning_on_first_large_build(oracle):
     plain = Context(0)
     try:
         plain.set_autotune(False)
+        # a single-job build never pays the timing passes
+        with build_conflict_graph(parts[0], 13, 6, ctx) as G:
+            assert G.edges > 0
+        assert ctx.work_split(LANES_BYTE) == (24, False)
         with build_batch(jobs, ctx) as A, build_batch(jobs, plain) as B:
             ra, ca = A.upper_csr()
             rb, cb = B.upper_csr()
