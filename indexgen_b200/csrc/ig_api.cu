@@ -290,6 +290,126 @@ bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int
     return !failed;
 }
 
+GreedyPool::GreedyPool(int threads)
+{
+    const int T = threads > 0 ? threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    for (int t = 0; t < T; ++t)
+        threads_.emplace_back([this]() { work(); });
+}
+
+GreedyPool::~GreedyPool()
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &th : threads_)
+        th.join();
+}
+
+void GreedyPool::submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts)
+{
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        for (int j = 0; j < (int)hg->jobs.size(); ++j) {
+            Task t;
+            t.edges = hg->job_edge_off[(size_t)j + 1] - hg->job_edge_off[(size_t)j];
+            t.seq = seq_++;
+            t.hg = hg;
+            t.job = j;
+            t.out = order + (hg->jobs[(size_t)j].word_off - order_base);
+            t.count = counts + j;
+            q_.push(std::move(t));
+        }
+    }
+    cv_.notify_all();
+}
+
+bool GreedyPool::wait()
+{
+    std::unique_lock<std::mutex> lk(mu_);
+    idle_.wait(lk, [this]() { return q_.empty() && busy_ == 0; });
+    return !failed_;
+}
+
+void GreedyPool::work()
+{
+    std::unique_lock<std::mutex> lk(mu_);
+    for (;;) {
+        cv_.wait(lk, [this]() { return stop_ || !q_.empty(); });
+        if (q_.empty())
+            return;  // stop_ and nothing left
+        Task t = q_.top();
+        q_.pop();
+        ++busy_;
+        lk.unlock();
+        bool ok = true;
+        try {
+            *t.count = greedy_one(*t.hg, t.job, t.out);
+        } catch (...) {
+            ok = false;
+        }
+        t.hg.reset();  // the last task of a graph frees its host copy here
+        lk.lock();
+        --busy_;
+        if (!ok)
+            failed_ = true;
+        if (q_.empty() && busy_ == 0)
+            idle_.notify_all();
+    }
+}
+
+// Pipeline: the batch is cut into up to eight contiguous groups of about
+// equal pair count; as soon as a group's graph is downloaded its jobs join the
+// greedy pool's queue (largest first), so host threads run the greedies of
+// every finished group while the device builds the next.
+ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, const int64_t *offsets, int32_t jobs,
+                       const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
+                       int32_t *order, int32_t *counts, int64_t *edges)
+{
+    long double total = 0;
+    for (int32_t j = 0; j < jobs; ++j)
+        total += (long double)(offsets[j + 1] - offsets[j]) * (offsets[j + 1] - offsets[j]);
+    const int groups = std::max(1, std::min<int>(8, jobs));
+    std::vector<int> cut{0};
+    long double acc = 0;
+    for (int32_t j = 0; j < jobs; ++j) {
+        acc += (long double)(offsets[j + 1] - offsets[j]) * (offsets[j + 1] - offsets[j]);
+        if ((int)cut.size() < groups && acc >= total * cut.size() / groups && j + 1 < jobs)
+            cut.push_back(j + 1);
+    }
+    cut.push_back(jobs);
+    ig_status s = IG_OK;
+    GreedyPool pool(host_threads);
+    for (size_t gi = 0; gi + 1 < cut.size(); ++gi) {
+        const int lo = cut[gi], hi = cut[gi + 1];
+        if (lo >= hi)
+            continue;
+        std::vector<int64_t> sub((size_t)(hi - lo) + 1);
+        for (int j = lo; j <= hi; ++j)
+            sub[(size_t)(j - lo)] = offsets[j] - offsets[lo];
+        ig_graph *g = nullptr;
+        s = ig_batch_build(ctx, words + offsets[lo], sub.data(), hi - lo, lens + lo, min_eds + lo, words_on_device,
+                           &g);
+        if (s != IG_OK)
+            break;
+        if (edges)
+            for (int j = lo; j < hi; ++j)
+                edges[j] = g->job_edge_off[(size_t)(j - lo) + 1] - g->job_edge_off[(size_t)(j - lo)];
+        auto hg = std::make_shared<HostGraph>();
+        s = download_for_greedy(g, order_threads, *hg);
+        release_graph(g);
+        if (s != IG_OK)
+            break;
+        pool.submit(hg, 0, order + offsets[lo], counts + lo);
+    }
+    const bool host_ok = pool.wait();
+    if (s == IG_OK && !host_ok)
+        s = set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
+    return s;
+}
+
 namespace {
 
 ig_status job_codebooks_impl(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
@@ -671,54 +791,8 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     ig_status s = ig::make_jobs(ctx, offsets, jobs, lens, min_eds, spec);
     if (s != IG_OK)
         return s;
-    // Pipeline: the batch is cut into up to four contiguous groups of about
-    // equal pair count; while the device builds group g+1, host threads run
-    // the greedies of group g.
-    long double total = 0;
-    for (const ig::JobSpec &j : spec)
-        total += (long double)j.n * j.n;
-    const int groups = std::max(1, std::min<int>(4, jobs));
-    std::vector<int> cut{0};
-    long double acc = 0;
-    for (int32_t j = 0; j < jobs; ++j) {
-        acc += (long double)spec[(size_t)j].n * spec[(size_t)j].n;
-        if ((int)cut.size() < groups && acc >= total * cut.size() / groups && j + 1 < jobs)
-            cut.push_back(j + 1);
-    }
-    cut.push_back(jobs);
-    std::thread host;
-    bool host_ok = true;
-    for (size_t gi = 0; gi + 1 < cut.size(); ++gi) {
-        const int lo = cut[gi], hi = cut[gi + 1];
-        if (lo >= hi)
-            continue;
-        std::vector<int64_t> sub((size_t)(hi - lo) + 1);
-        for (int j = lo; j <= hi; ++j)
-            sub[(size_t)(j - lo)] = offsets[j] - offsets[lo];
-        ig_graph *g = nullptr;
-        s = ig_batch_build(ctx, words + offsets[lo], sub.data(), hi - lo, lens + lo, min_eds + lo, 0, &g);
-        if (s != IG_OK)
-            break;
-        if (edges)
-            for (int j = lo; j < hi; ++j)
-                edges[j] = g->job_edge_off[(size_t)(j - lo) + 1] - g->job_edge_off[(size_t)(j - lo)];
-        auto hg = std::make_shared<ig::HostGraph>();
-        s = ig::download_for_greedy(g, order_threads, *hg);
-        ig::release_graph(g);
-        if (s != IG_OK)
-            break;
-        if (host.joinable())
-            host.join();
-        host = std::thread([hg, host_threads, order, counts, lo, off = offsets[lo], &host_ok]() {
-            if (!ig::run_greedies(*hg, host_threads, 0, order + off, counts + lo))
-                host_ok = false;
-        });
-    }
-    if (host.joinable())
-        host.join();
-    if (s == IG_OK && !host_ok)
-        s = ig::set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
-    return s;
+    return ig::solve_groups(ctx, words, 0, offsets, jobs, lens, min_eds, order_threads, host_threads, order, counts,
+                            edges);
 }
 
 ig_status ig_graph_write_adj_list(ig_graph *g, const char *path, int64_t *bytes)

@@ -187,21 +187,14 @@ extern "C" ig_status ig_cluster_solve(ig_ctx *ctx, const uint32_t *words, int32_
             if (s != IG_OK)
                 return s;
         }
-        // all clusters in one batch; greedies on host threads
+        // all clusters as one pipelined batch: groups built on the device
+        // while host threads run the greedies of the groups already built
         std::vector<int32_t> lens((size_t)jobs, len), eds((size_t)jobs, min_ed), counts((size_t)jobs, 0);
         std::vector<int32_t> order((size_t)N, 0);
-        ig_graph *g = nullptr;
-        ig_status s = ig_batch_build(ctx, static_cast<const uint32_t *>(d_part.p), offs.data(), jobs, lens.data(),
-                                     eds.data(), 1, &g);
+        ig_status s = solve_groups(ctx, static_cast<const uint32_t *>(d_part.p), 1, offs.data(), jobs, lens.data(),
+                                   eds.data(), 1, host_threads, order.data(), counts.data(), nullptr);
         if (s != IG_OK)
             return s;
-        HostGraph hg;
-        s = download_for_greedy(g, 1, hg);
-        ig_graph_free(g);
-        if (s != IG_OK)
-            return s;
-        if (!run_greedies(hg, host_threads, 0, order.data(), counts.data()))
-            return set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
         next.clear();
         for (int32_t j = 0; j < jobs; ++j)
             for (int32_t q = 0; q < counts[(size_t)j]; ++q)

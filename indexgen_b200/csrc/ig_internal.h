@@ -5,6 +5,9 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <queue>
+#include <condition_variable>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -206,6 +209,50 @@ ig_status download_for_greedy(Graph *g, int order_threads, HostGraph &hg);
 bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts);
 // Greedy of one job of a downloaded graph into out (job-local ids).
 int32_t greedy_one(const HostGraph &hg, int job, int32_t *out);
+
+// Builds the jobs (words [offsets[j], offsets[j+1]), host or device pointer)
+// in up to eight groups and runs their greedies on host_threads threads as
+// each group arrives; job j's selection goes to order + offsets[j], its size
+// to counts[j], its edge count to edges[j] (optional).  Jobs must be valid
+// (ig_api.cu).
+ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, const int64_t *offsets, int32_t jobs,
+                       const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
+                       int32_t *order, int32_t *counts, int64_t *edges);
+
+// Host threads that run job greedies as downloaded graphs arrive: tasks of
+// all submitted graphs share one queue, largest (most edges) first, so the
+// greedies of a batch group start while the device builds the next group and
+// idle threads take jobs of any group (ig_api.cu).
+class GreedyPool {
+  public:
+    explicit GreedyPool(int threads);
+    ~GreedyPool();  // waits for the queued jobs
+    // Queues every job of hg: job j's selection goes to order + word_off_j -
+    // order_base, its size to counts[j].
+    void submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts);
+    // Waits until the queue is empty and every task has finished; false if a
+    // greedy failed to allocate.
+    bool wait();
+
+  private:
+    struct Task {
+        int64_t edges;
+        int64_t seq;
+        std::shared_ptr<const HostGraph> hg;
+        int job;
+        int32_t *out;
+        int32_t *count;
+        bool operator<(const Task &o) const { return edges != o.edges ? edges < o.edges : seq > o.seq; }
+    };
+    void work();
+    std::mutex mu_;
+    std::condition_variable cv_, idle_;
+    std::priority_queue<Task> q_;
+    std::vector<std::thread> threads_;
+    int64_t seq_ = 0;
+    int busy_ = 0;
+    bool stop_ = false, failed_ = false;
+};
 
 // Makes a device current for the duration of a call and restores the
 // caller's device afterwards.
