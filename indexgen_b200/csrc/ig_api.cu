@@ -381,7 +381,8 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
     }
     cut.push_back(jobs);
     ig_status s = IG_OK;
-    GreedyPool pool(host_threads);
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    GreedyPool pool(std::max(1, std::min<int>(host_threads > 0 ? host_threads : hw, jobs)));
     for (size_t gi = 0; gi + 1 < cut.size(); ++gi) {
         const int lo = cut[gi], hi = cut[gi + 1];
         if (lo >= hi)
