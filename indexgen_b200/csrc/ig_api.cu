@@ -142,6 +142,69 @@ ig_status fetch_adjacency(ig_graph *g, HostGraph &hg)
     return IG_OK;
 }
 
+// fetch_adjacency with the copy on the context's download stream: returns
+// once the copy is queued, followed by the host function `then(arg)` (run by
+// the CUDA runtime when the copy has landed; it must not call CUDA) and the
+// event *done.  The caller may queue more work on the context stream
+// meanwhile (the next batch group's build overlaps the copy) and must wait on
+// *done before it frees g.  On an error nothing of `then` runs.
+ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, cudaHostFn_t then, void *arg)
+{
+    ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    ig_status s = build_adjacency(ctx, g);  // ends with the context stream idle
+    if (s != IG_OK)
+        return s;
+    cudaError_t e = cudaSuccess;
+    if (!ctx->dl_stream && (e = cudaStreamCreateWithFlags(&ctx->dl_stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        ctx->dl_stream = nullptr;
+        return cuda_error(ctx, e, "download stream");
+    }
+    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
+    const size_t adj_bytes = (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
+    std::shared_ptr<void> block = ctx->pinned->acquire(ptr_bytes + adj_bytes);
+    if (!block) {
+        void *p = std::malloc(ptr_bytes + adj_bytes);
+        if (!p)
+            return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
+        block = std::shared_ptr<void>(p, std::free);
+    }
+    int64_t *ap = static_cast<int64_t *>(block.get());
+    int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
+    cudaEvent_t fin = nullptr;
+    if ((e = cudaEventCreateWithFlags(&fin, cudaEventDisableTiming)) != cudaSuccess)
+        return cuda_error(ctx, e, "download event");
+    e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, ctx->dl_stream);
+    if (e == cudaSuccess && g->edges > 0)
+        e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            ctx->dl_stream);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(ctx->dl_stream);
+        cudaEventDestroy(fin);
+        return cuda_error(ctx, e, "adjacency download");
+    }
+    hg.order_threads = 1;
+    hg.jobs = g->jobs;
+    hg.job_edge_off = g->job_edge_off;
+    hg.ptr = ap;
+    hg.idx = adj;
+    hg.storage = std::move(block);
+    if (then && (e = cudaLaunchHostFunc(ctx->dl_stream, then, arg)) != cudaSuccess) {
+        cudaStreamSynchronize(ctx->dl_stream);
+        cudaEventDestroy(fin);
+        return cuda_error(ctx, e, "download callback");
+    }
+    if ((e = cudaEventRecord(fin, ctx->dl_stream)) != cudaSuccess) {
+        cudaStreamSynchronize(ctx->dl_stream);  // `then` has run
+        cudaEventDestroy(fin);
+        *done = nullptr;
+        return IG_OK;
+    }
+    *done = fin;
+    return IG_OK;
+}
+
 // Validated job list from an offsets array.
 ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *lens, const int32_t *min_eds,
                     std::vector<JobSpec> &jobs)
@@ -360,6 +423,19 @@ void GreedyPool::work()
     }
 }
 
+// Host callback of a group's adjacency copy: queues the group's greedies.
+struct SubmitWhenCopied {
+    GreedyPool *pool;
+    std::shared_ptr<HostGraph> hg;
+    int32_t *order;
+    int32_t *counts;
+    static void CUDART_CB run(void *p)
+    {
+        std::unique_ptr<SubmitWhenCopied> c(static_cast<SubmitWhenCopied *>(p));
+        c->pool->submit(c->hg, 0, c->order, c->counts);
+    }
+};
+
 // Pipeline: the batch is cut into up to eight contiguous groups of about
 // equal pair count; as soon as a group's graph is downloaded its jobs join the
 // greedy pool's queue (largest first), so host threads run the greedies of
@@ -383,6 +459,28 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
     ig_status s = IG_OK;
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     GreedyPool pool(std::max(1, std::min<int>(host_threads > 0 ? host_threads : hw, jobs)));
+    // A group whose adjacency copy runs on the download stream while the
+    // next group builds; the copy's host callback queues its greedies the
+    // moment it lands, and the group's device buffers are freed after the
+    // next build.
+    struct Pending {
+        ig_graph *g = nullptr;
+        cudaEvent_t done = nullptr;
+    } pend;
+    auto finish = [&]() -> ig_status {
+        if (!pend.g)
+            return IG_OK;
+        ig_status r = IG_OK;
+        if (pend.done) {
+            const cudaError_t e = cudaEventSynchronize(pend.done);
+            cudaEventDestroy(pend.done);
+            if (e != cudaSuccess)
+                r = cuda_error(ctx, e, "adjacency download");
+        }
+        release_graph(pend.g);
+        pend = Pending();
+        return r;
+    };
     for (size_t gi = 0; gi + 1 < cut.size(); ++gi) {
         const int lo = cut[gi], hi = cut[gi + 1];
         if (lo >= hi)
@@ -393,18 +491,39 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
         ig_graph *g = nullptr;
         s = ig_batch_build(ctx, words + offsets[lo], sub.data(), hi - lo, lens + lo, min_eds + lo, words_on_device,
                            &g);
-        if (s != IG_OK)
+        const ig_status f = finish();  // the previous group's copy ran during this build
+        if (s == IG_OK)
+            s = f;
+        if (s != IG_OK) {
+            release_graph(g);
             break;
+        }
         if (edges)
             for (int j = lo; j < hi; ++j)
                 edges[j] = g->job_edge_off[(size_t)(j - lo) + 1] - g->job_edge_off[(size_t)(j - lo)];
         auto hg = std::make_shared<HostGraph>();
-        s = download_for_greedy(g, order_threads, *hg);
-        release_graph(g);
-        if (s != IG_OK)
-            break;
-        pool.submit(hg, 0, order + offsets[lo], counts + lo);
+        if (order_threads == 1) {
+            cudaEvent_t done = nullptr;
+            auto *sub_ctx = new SubmitWhenCopied{&pool, hg, order + offsets[lo], counts + lo};
+            s = fetch_adjacency_async(g, *hg, &done, SubmitWhenCopied::run, sub_ctx);
+            if (s != IG_OK) {
+                delete sub_ctx;
+                release_graph(g);
+                break;
+            }
+            pend.g = g;
+            pend.done = done;
+        } else {
+            s = download_for_greedy(g, order_threads, *hg);
+            release_graph(g);
+            if (s != IG_OK)
+                break;
+            pool.submit(hg, 0, order + offsets[lo], counts + lo);
+        }
     }
+    const ig_status f = finish();
+    if (s == IG_OK)
+        s = f;
     const bool host_ok = pool.wait();
     if (s == IG_OK && !host_ok)
         s = set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
@@ -500,6 +619,10 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
         for (cudaGraphExec_t x : ctx->graph_exec)
             if (x)
                 cudaGraphExecDestroy(x);
+        if (ctx->dl_stream) {
+            cudaStreamSynchronize(ctx->dl_stream);
+            cudaStreamDestroy(ctx->dl_stream);
+        }
         if (ctx->stage)
             cudaFreeHost(ctx->stage);
         cudaGetLastError();

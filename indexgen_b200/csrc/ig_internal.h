@@ -110,6 +110,8 @@ struct Ctx {
     cudaGraphExec_t graph_exec[2] = {};
     std::vector<uint64_t> graph_sig[2];  // arguments baked into each cached graph
     int64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
+    // second stream for device-to-host copies that overlap the next build
+    cudaStream_t dl_stream = nullptr;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
     size_t stage_bytes = 0;
