@@ -1107,7 +1107,8 @@ ig_status ensure_stage(Ctx *ctx, size_t bytes)
 // arguments, grids and copy addresses differ between batches) or
 // instantiated afresh, and the executable graph is launched on the stream.
 // With graphs off, or with per-phase event timing on (events recorded inside
-// a capture are not timed), the calls run directly on the stream.
+// a capture are not timed), the calls run directly on the stream; so they do
+// for good on a context where capturing or instantiating failed.
 //
 // `sig` lists every pointer, size, grid and scalar argument the calls bake
 // into the graph (not the contents of the staging block, which the graph's
@@ -1129,9 +1130,17 @@ ig_status run_graph(Ctx *ctx, int slot, const std::vector<uint64_t> &sig, const 
         return IG_OK;
     }
     ctx->graph_sig[slot].clear();
+    // Nothing captured has run, so when the graph machinery itself fails the
+    // context turns graphs off and queues the same calls directly.
+    auto direct = [&]() -> ig_status {
+        cudaGetLastError();
+        ctx->use_graphs = false;
+        const cudaError_t de = enqueue();
+        return de == cudaSuccess ? IG_OK : cuda_error(ctx, de, what);
+    };
     cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess)
-        return cuda_error(ctx, e, what);
+        return direct();
     const cudaError_t qe = enqueue();
     cudaGraph_t graph = nullptr;
     e = cudaStreamEndCapture(st, &graph);
@@ -1139,7 +1148,9 @@ ig_status run_graph(Ctx *ctx, int slot, const std::vector<uint64_t> &sig, const 
         if (graph)
             cudaGraphDestroy(graph);
         cudaGetLastError();
-        return cuda_error(ctx, qe != cudaSuccess ? qe : e, what);
+        if (qe != cudaSuccess && qe != cudaErrorStreamCaptureUnsupported && qe != cudaErrorStreamCaptureInvalidated)
+            return cuda_error(ctx, qe, what);  // a launch error of the calls themselves
+        return direct();
     }
     cudaGraphExec_t &exec = ctx->graph_exec[slot];
     if (exec) {
@@ -1157,7 +1168,7 @@ ig_status run_graph(Ctx *ctx, int slot, const std::vector<uint64_t> &sig, const 
         if (e != cudaSuccess) {
             exec = nullptr;
             cudaGraphDestroy(graph);
-            return cuda_error(ctx, e, what);
+            return direct();
         }
         ctx->graph_instantiations++;
     }
@@ -1362,6 +1373,7 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
         (uint64_t)sgrid,             (uint64_t)(uintptr_t)ctx->scan_tmp.ptr};
     int64_t launched = 0;
     s = run_graph(ctx, out ? 0 : 1, sig, out ? "build pass" : "count pass", [&]() -> cudaError_t {
+        launched = 0;
         cudaError_t e = cudaMemcpyAsync(jbase, stage, table, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess)
             return e;
