@@ -437,7 +437,7 @@ struct SubmitWhenCopied {
 };
 
 // Pipeline: the batch is cut into up to eight contiguous groups of about
-// equal pair count; as soon as a group's graph is downloaded its jobs join the
+// equal pair count (at least 2^30 pair tests each); as soon as a group's graph is downloaded its jobs join the
 // greedy pool's queue (largest first), so host threads run the greedies of
 // every finished group while the device builds the next.
 ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, const int64_t *offsets, int32_t jobs,
@@ -447,7 +447,11 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
     long double total = 0;
     for (int32_t j = 0; j < jobs; ++j)
         total += (long double)(offsets[j + 1] - offsets[j]) * (offsets[j + 1] - offsets[j]);
-    const int groups = std::max(1, std::min<int>(8, jobs));
+    // a group costs a few hundred microseconds of host round trips besides
+    // its device work, so each one gets at least 2^30 pair tests (about
+    // 1.4 ms on nibble lanes): small batches stay one launch
+    const long double min_group = (long double)(1ull << 31);  // total counts n^2, not n(n-1)/2
+    const int groups = (int)std::max<long double>(1, std::min<long double>({8.0L, (long double)jobs, total / min_group}));
     std::vector<int> cut{0};
     long double acc = 0;
     for (int32_t j = 0; j < jobs; ++j) {
@@ -457,8 +461,11 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
     }
     cut.push_back(jobs);
     ig_status s = IG_OK;
+    // One core stays with this thread: it drives the device, and a build
+    // that waits for a core behind the greedies stalls the whole pipeline.
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
-    GreedyPool pool(std::max(1, std::min<int>(host_threads > 0 ? host_threads : hw, jobs)));
+    const int cap = std::max(1, hw - 1);
+    GreedyPool pool(std::max(1, std::min({host_threads > 0 ? host_threads : cap, cap, (int)jobs})));
     // A group whose adjacency copy runs on the download stream while the
     // next group builds; the copy's host callback queues its greedies the
     // moment it lands, and the group's device buffers are freed after the
