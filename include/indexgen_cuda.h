@@ -186,7 +186,12 @@ ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word
  * is written to order + offsets[j]; counts[j] is its size.  order_threads as
  * in ig_graph_codebook. */
 ig_status ig_graph_job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts);
-/* Build + job codebooks in one call; edges[j] (optional) = edges of job j. */
+/* Build + job codebooks in one call; edges[j] (optional) = edges of job j.
+ * The jobs are built in up to eight groups (at least 2^30 pair tests each);
+ * each group's greedies start on the host as soon as its adjacency has been
+ * copied, while the device builds the next group.  Greedy threads: at most
+ * host_threads (0 = all cores), and always one fewer than the cores, so the
+ * thread that drives the device is never starved. */
 ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
                          const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
                          int32_t *order, int32_t *counts, int64_t *edges);
@@ -202,7 +207,8 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
  * in the reference, which solves one job per program run. */
 typedef struct ig_server ig_server;
 typedef struct ig_server_opts {
-    int host_threads;          /* greedy threads (0 = all cores)                  */
+    int host_threads;          /* greedy threads (0 = all cores; at most cores - 1,
+                                * leaving one to the scheduler)                  */
     int max_batch_jobs;        /* jobs per launch (0 = 256)                       */
     int order_threads;         /* neighbour order (0 or 1 = canonical sorted)     */
     int reserved;

@@ -216,8 +216,12 @@ ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **
     ig_server_opts o{};
     if (opts)
         o = *opts;
+    // greedy threads leave one core to the scheduler thread, which drives the
+    // device: a build that waits for a core stalls every job behind it
+    const int cores = (int)std::max(1u, std::thread::hardware_concurrency());
     if (o.host_threads <= 0)
-        o.host_threads = (int)std::max(1u, std::thread::hardware_concurrency());
+        o.host_threads = cores;
+    o.host_threads = std::max(1, std::min(o.host_threads, cores - 1));
     if (o.max_batch_jobs <= 0)
         o.max_batch_jobs = 256;
     if (o.max_batch_pairs <= 0)

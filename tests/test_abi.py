@@ -132,3 +132,25 @@ def test_ctx_create_without_gpu_fails_cleanly(L):
     st = L.ig_ctx_create(ctypes.byref(h), 0)
     assert st != 0 and not h.value
     assert L.ig_ctx_create(None, 0) == 1
+
+
+def test_lane_forms_and_null_context_calls(L):
+    """Lane form per (len, min_ed) (host only) and the tuning / graph calls'
+    argument checks, which need no device."""
+    from indexgen_b200 import LANES_BYTE, LANES_FULL, LANES_NIBBLE, lane_form
+
+    for d in range(1, 5):
+        assert lane_form(12, d) == LANES_NIBBLE
+    for d in range(5, 9):
+        assert lane_form(16, d) == LANES_BYTE
+    assert lane_form(16, 9) == LANES_FULL and lane_form(10, 0) == LANES_FULL
+    assert lane_form(0, 4) == -1 and lane_form(17, 4) == -1
+    v = ctypes.c_int32()
+    t = ctypes.c_int()
+    n = ctypes.c_int64()
+    assert L.ig_ctx_autotune(None, None, 0, 12, 4, 0, ctypes.byref(v)) == 1
+    assert L.ig_ctx_set_work_split(None, 1, 24) == 1
+    assert L.ig_ctx_work_split(None, 1, ctypes.byref(v), ctypes.byref(t)) == 1
+    assert L.ig_ctx_set_autotune(None, 1) == 1
+    assert L.ig_ctx_set_graphs(None, 1) == 1
+    assert L.ig_ctx_graph_stats(None, ctypes.byref(n), None, None) == 1
