@@ -615,7 +615,7 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
         ig::DeviceGuard dg(ctx->device);
         for (ig::DevBuf *b :
              {&ctx->words, &ctx->sel, &ctx->counts, &ctx->records, &ctx->scan_tmp, &ctx->flags, &ctx->adj_tmp,
-              &ctx->jobs, &ctx->aux})
+              &ctx->jobs, &ctx->aux, &ctx->cols_ws})
             if (b->ptr)
                 cudaFreeAsync(b->ptr, ctx->stream);
         cudaStreamSynchronize(ctx->stream);

@@ -1729,22 +1729,23 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     }
     unsigned long long slots = 0, total = 0;
     for (int attempt = 0;; ++attempt) {
-        // columns: room for every record slot the pass may fill (at most one
-        // per pair test), so the compaction runs in the same graph as the
-        // pair kernels, before the host has seen the edge count
+        // columns go to a context workspace with room for every record slot
+        // the pass may fill (at most one per pair test), so the compaction
+        // runs in the same graph as the pair kernels, before the host has
+        // seen the edge count; the graph then gets an exact copy
         const size_t col_cap = (size_t)std::min<unsigned long long>(ctx->rec_capacity, (unsigned long long)B.pairs);
-        IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>(col_cap, 1) * sizeof(int32_t), st));
+        if ((s = ensure(ctx, ctx->cols_ws, std::max<size_t>(col_cap, 1) * sizeof(int32_t), "column workspace")) !=
+            IG_OK)
+            return s;
         CompactOut out;
         out.row_ptr = g->d_row_ptr;
-        out.cols = g->d_cols;
+        out.cols = static_cast<int32_t *>(ctx->cols_ws.ptr);
         out.n = n;
         s = run_pass(ctx, d_words, B, grid, &out, &slots, &total, g->job_edge_off.data());
         if (s != IG_OK)
             return s;
         if (slots <= ctx->rec_capacity)
             break;
-        cudaFreeAsync(g->d_cols, st);
-        g->d_cols = nullptr;
         if (attempt > 0)
             return set_error(ctx, IG_ERR_STATE, "record slots exceeded a buffer sized for them twice");
         // slots of a rerun differ from this pass only by the chunk tails of
@@ -1761,6 +1762,12 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     const int njobs = (int)B.desc.size();
     if (g->job_edge_off[(size_t)njobs] != (int64_t)total)
         return set_error(ctx, IG_ERR_STATE, "row offsets disagree with the edge count");
+    IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
+    if (total > 0) {
+        IG_CUDA(cudaMemcpyAsync(g->d_cols, ctx->cols_ws.ptr, (size_t)total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
+                                st));
+        IG_CUDA(cudaStreamSynchronize(st));
+    }
     return IG_OK;
 }
 

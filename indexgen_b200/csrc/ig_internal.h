@@ -83,7 +83,7 @@ struct Ctx {
     std::string last_error;
     int64_t launches = 0;
     // workspace
-    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs, aux;
+    DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs, aux, cols_ws;
     unsigned long long rec_capacity = 0;  // records that fit in `records`
     int pair_grid = 0;                    // persistent CTAs of the pair kernel
     int pair_grid_nib = 0;                // ... of the nibble-lane pair kernel
