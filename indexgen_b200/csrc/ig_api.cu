@@ -391,9 +391,34 @@ void GreedyPool::submit(std::shared_ptr<const HostGraph> hg, int64_t order_base,
 
 bool GreedyPool::wait()
 {
+    // the waiting thread is done driving the device: it runs queued
+    // greedies too, then waits for the ones in flight
     std::unique_lock<std::mutex> lk(mu_);
+    while (!q_.empty())
+        run_one(lk);
     idle_.wait(lk, [this]() { return q_.empty() && busy_ == 0; });
     return !failed_;
+}
+
+void GreedyPool::run_one(std::unique_lock<std::mutex> &lk)
+{
+    Task t = q_.top();
+    q_.pop();
+    ++busy_;
+    lk.unlock();
+    bool ok = true;
+    try {
+        *t.count = greedy_one(*t.hg, t.job, t.out);
+    } catch (...) {
+        ok = false;
+    }
+    t.hg.reset();  // the last task of a graph frees its host copy here
+    lk.lock();
+    --busy_;
+    if (!ok)
+        failed_ = true;
+    if (q_.empty() && busy_ == 0)
+        idle_.notify_all();
 }
 
 void GreedyPool::work()
@@ -403,23 +428,7 @@ void GreedyPool::work()
         cv_.wait(lk, [this]() { return stop_ || !q_.empty(); });
         if (q_.empty())
             return;  // stop_ and nothing left
-        Task t = q_.top();
-        q_.pop();
-        ++busy_;
-        lk.unlock();
-        bool ok = true;
-        try {
-            *t.count = greedy_one(*t.hg, t.job, t.out);
-        } catch (...) {
-            ok = false;
-        }
-        t.hg.reset();  // the last task of a graph frees its host copy here
-        lk.lock();
-        --busy_;
-        if (!ok)
-            failed_ = true;
-        if (q_.empty() && busy_ == 0)
-            idle_.notify_all();
+        run_one(lk);
     }
 }
 

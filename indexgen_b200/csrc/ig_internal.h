@@ -232,8 +232,8 @@ class GreedyPool {
     // Queues every job of hg: job j's selection goes to order + word_off_j -
     // order_base, its size to counts[j].
     void submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts);
-    // Waits until the queue is empty and every task has finished; false if a
-    // greedy failed to allocate.
+    // Runs queued greedies on the calling thread too until the queue is
+    // empty, then waits for the rest; false if a greedy failed to allocate.
     bool wait();
 
   private:
@@ -247,6 +247,7 @@ class GreedyPool {
         bool operator<(const Task &o) const { return edges != o.edges ? edges < o.edges : seq > o.seq; }
     };
     void work();
+    void run_one(std::unique_lock<std::mutex> &lk);  // pops the top task; lk held on entry and exit
     std::mutex mu_;
     std::condition_variable cv_, idle_;
     std::priority_queue<Task> q_;
