@@ -914,8 +914,22 @@ __global__ void row_prefix(uint32_t *__restrict__ counts, const JobDesc *__restr
     const int64_t row = gr - J.word_off;
     const int g = (int)(((row / kBandRows) * kBandRows) >> J.seg_shift);
     uint32_t acc = 0;
-    for (int s = g; s < J.nseg; ++s) {
-        uint32_t *p = counts + J.count_off + (int64_t)s * J.n + row;
+    uint32_t *p = counts + J.count_off + (int64_t)g * J.n + row;
+    int s = g;
+    // eight cells per round, loaded before any is rewritten, so a thread keeps
+    // eight DRAM reads in flight instead of one
+    for (; s + 8 <= J.nseg; s += 8, p += 8 * (int64_t)J.n) {
+        uint32_t c[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            c[k] = p[(int64_t)k * J.n];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            p[(int64_t)k * J.n] = acc;
+            acc += c[k];
+        }
+    }
+    for (; s < J.nseg; ++s, p += J.n) {
         const uint32_t c = *p;
         *p = acc;
         acc += c;
