@@ -1776,6 +1776,15 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     const int njobs = (int)B.desc.size();
     if (g->job_edge_off[(size_t)njobs] != (int64_t)total)
         return set_error(ctx, IG_ERR_STATE, "row offsets disagree with the edge count");
+    if ((size_t)total * sizeof(int32_t) * 2 >= ctx->cols_ws.bytes) {
+        // the columns fill most of the workspace: the graph takes it over
+        // (no copy, no second array of that size) and the next build
+        // allocates a new one
+        g->d_cols = static_cast<int32_t *>(ctx->cols_ws.ptr);
+        ctx->cols_ws.ptr = nullptr;
+        ctx->cols_ws.bytes = 0;
+        return IG_OK;
+    }
     IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
     if (total > 0) {
         IG_CUDA(cudaMemcpyAsync(g->d_cols, ctx->cols_ws.ptr, (size_t)total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
