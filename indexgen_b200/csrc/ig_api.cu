@@ -63,11 +63,16 @@ ig_status stage_words(Ctx *ctx, const uint32_t *words, int32_t n, int on_device,
     return IG_OK;
 }
 
-void release_graph(ig_graph *g)
+void release_graph(ig_graph *g, bool caller_holds_lock = false)
 {
     if (!g)
         return;
     if (g->ctx) {
+        // the frees go on the context stream: under the context lock, so that
+        // they never land inside another thread's graph capture of that stream
+        std::unique_lock<std::mutex> lk(g->ctx->mu, std::defer_lock);
+        if (!caller_holds_lock)
+            lk.lock();
         DeviceGuard dg(g->ctx->device);
         if (g->d_row_ptr)
             cudaFreeAsync(g->d_row_ptr, g->ctx->stream);
@@ -87,6 +92,7 @@ ig_status fetch_host(ig_graph *g)
     if (g->host_valid)
         return IG_OK;
     ig::Ctx *ctx = g->ctx;
+    std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     try {
         g->h_row_ptr.resize((size_t)g->n + 1);
@@ -732,7 +738,7 @@ ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len,
     if (s == IG_OK)
         s = ig::build_batch(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, g);
     if (s != IG_OK) {
-        ig::release_graph(g);
+        ig::release_graph(g, true);
         return s;
     }
     *out = g;
@@ -914,7 +920,7 @@ ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     if (s == IG_OK)
         s = ig::build_batch(ctx, d_words, spec, g);
     if (s != IG_OK) {
-        ig::release_graph(g);
+        ig::release_graph(g, true);
         return s;
     }
     *out = g;
@@ -961,7 +967,7 @@ ig_status ig_graph_read_adj_list(ig_ctx *ctx, const char *path, ig_graph **out)
         return IG_ERR_OOM;
     const ig_status s = ig::read_adj_list(ctx, path, g);
     if (s != IG_OK) {
-        ig::release_graph(g);
+        ig::release_graph(g, true);
         return s;
     }
     *out = g;
