@@ -148,6 +148,28 @@ ig_status fetch_adjacency(ig_graph *g, HostGraph &hg)
     return IG_OK;
 }
 
+// Validated job list from an offsets array.
+ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *lens, const int32_t *min_eds,
+                    std::vector<JobSpec> &jobs)
+{
+    if (k < 0 || (k > 0 && (!offsets || !lens || !min_eds)))
+        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[k+1], lens[k] and min_eds[k] are required");
+    if (k > 0 && offsets[0] != 0)
+        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[0] must be 0");
+    jobs.clear();
+    for (int32_t j = 0; j < k; ++j) {
+        const int64_t n = offsets[j + 1] - offsets[j];
+        if (n < 0 || n > INT32_MAX || lens[j] < 1 || lens[j] > IG_MAX_LEN)
+            return set_error(ctx, IG_ERR_INPUT, "jobs: offsets must not decrease and 1 <= len <= 16");
+        jobs.push_back(JobSpec{offsets[j], (int32_t)n, lens[j], min_eds[j]});
+    }
+    if (k > 0 && offsets[k] > INT32_MAX)
+        return set_error(ctx, IG_ERR_CAPACITY, "more than 2^31-1 words in one batch");
+    return IG_OK;
+}
+
+}  // namespace
+
 // fetch_adjacency with the copy on the context's download stream: returns
 // once the copy is queued, followed by the host function `then(arg)` (run by
 // the CUDA runtime when the copy has landed; it must not call CUDA) and the
@@ -211,27 +233,6 @@ ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, c
     return IG_OK;
 }
 
-// Validated job list from an offsets array.
-ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *lens, const int32_t *min_eds,
-                    std::vector<JobSpec> &jobs)
-{
-    if (k < 0 || (k > 0 && (!offsets || !lens || !min_eds)))
-        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[k+1], lens[k] and min_eds[k] are required");
-    if (k > 0 && offsets[0] != 0)
-        return set_error(ctx, IG_ERR_INPUT, "jobs: offsets[0] must be 0");
-    jobs.clear();
-    for (int32_t j = 0; j < k; ++j) {
-        const int64_t n = offsets[j + 1] - offsets[j];
-        if (n < 0 || n > INT32_MAX || lens[j] < 1 || lens[j] > IG_MAX_LEN)
-            return set_error(ctx, IG_ERR_INPUT, "jobs: offsets must not decrease and 1 <= len <= 16");
-        jobs.push_back(JobSpec{offsets[j], (int32_t)n, lens[j], min_eds[j]});
-    }
-    if (k > 0 && offsets[k] > INT32_MAX)
-        return set_error(ctx, IG_ERR_CAPACITY, "more than 2^31-1 words in one batch");
-    return IG_OK;
-}
-
-}  // namespace
 
 bool reserve_pool(Ctx *ctx, size_t bytes)
 {

@@ -206,6 +206,12 @@ struct HostGraph {
 };
 // Device -> host (ig_api.cu); the graph stays valid.
 ig_status download_for_greedy(Graph *g, int order_threads, HostGraph &hg);
+// The canonical adjacency (order_threads = 1) built on the device and copied
+// on the context's download stream, followed by the host function then(arg)
+// (run when the copy has landed; it must not call CUDA) and the event *done
+// (null when the copy has already completed).  The caller waits on *done
+// before it frees g (ig_api.cu).
+ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, cudaHostFn_t then, void *arg);
 // Greedy of every job on host threads, largest first; job j's selection goes
 // to order + word_off_j - order_base.  False on allocation failure.
 bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts);

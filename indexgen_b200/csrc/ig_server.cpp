@@ -8,9 +8,11 @@
 //                     long as the batch stays within the HBM budget (footprint
 //                     estimated per job) and the per-launch pair budget; builds
 //                     all their graphs with one device pipeline (one persistent
-//                     pair-test launch); downloads the canonical adjacency; hands
-//                     the jobs to the greedy pool; and immediately admits the
-//                     jobs that arrived meanwhile.
+//                     pair-test launch); queues the canonical adjacency's copy
+//                     to the host on a second stream, behind which a host
+//                     callback hands the jobs to the greedy pool; and
+//                     immediately admits the jobs that arrived meanwhile, whose
+//                     build overlaps that copy.
 //   greedy pool       host threads run each job's greedy while the device works
 //                     on the next batch; a job is done when its greedy is.
 // A job's result does not depend on what it was batched with: its graph is a
@@ -97,15 +99,56 @@ struct ig_server {
     void greedy_loop();
 };
 
+// Host callback behind a batch's adjacency copy: the batch's jobs go to the
+// greedy pool the moment their adjacency has landed (no CUDA calls here).
+struct BatchDelivery {
+    ig_server *sv;
+    std::shared_ptr<ig::HostGraph> hg;
+    std::vector<std::shared_ptr<ServerJob>> batch;
+    static void CUDART_CB run(void *p)
+    {
+        std::unique_ptr<BatchDelivery> d(static_cast<BatchDelivery *>(p));
+        std::lock_guard<std::mutex> lk(d->sv->mu);
+        for (size_t b = 0; b < d->batch.size(); ++b) {
+            d->batch[b]->state = kGreedy;
+            d->sv->tasks.push_back(GreedyTask{d->hg, (int)b, d->batch[b]});
+        }
+        d->sv->cv_tasks.notify_all();
+    }
+};
+
 void ig_server::schedule_loop()
 {
+    // the previous batch: its adjacency copy overlaps this batch's build, and
+    // its device graph is freed once the copy is done
+    ig_graph *pend_g = nullptr;
+    cudaEvent_t pend_done = nullptr;
+    auto finish_pending = [&]() {
+        if (!pend_g)
+            return;
+        if (pend_done) {
+            cudaEventSynchronize(pend_done);
+            cudaEventDestroy(pend_done);
+        }
+        ig_graph_free(pend_g);
+        pend_g = nullptr;
+        pend_done = nullptr;
+    };
     for (;;) {
         std::vector<std::shared_ptr<ServerJob>> batch;
         {
             std::unique_lock<std::mutex> lk(mu);
+            if (queue.empty() && pend_g) {  // nothing to overlap with: settle the last batch
+                lk.unlock();
+                finish_pending();
+                lk.lock();
+            }
             cv_queue.wait(lk, [&] { return stopping || !queue.empty(); });
-            if (stopping && queue.empty())
+            if (stopping && queue.empty()) {
+                lk.unlock();
+                finish_pending();
                 return;
+            }
             int64_t mem = 0;
             long double pairs = 0;
             while (!queue.empty()) {
@@ -140,8 +183,25 @@ void ig_server::schedule_loop()
         ig_graph *g = nullptr;
         ig_status s = ig_batch_build(ctx, words.data(), off.data(), (int32_t)batch.size(), lens.data(), eds.data(), 0,
                                      &g);
+        finish_pending();  // the previous batch's copy ran during this build
         auto hg = std::make_shared<ig::HostGraph>();
-        if (s == IG_OK) {
+        if (s == IG_OK && opts.order_threads == 1) {
+            for (size_t b = 0; b < batch.size(); ++b)
+                batch[b]->edges = g->job_edge_off[b + 1] - g->job_edge_off[b];
+            auto *d = new BatchDelivery{this, hg, batch};
+            cudaEvent_t done = nullptr;
+            s = ig::fetch_adjacency_async(g, *hg, &done, BatchDelivery::run, d);
+            if (s == IG_OK) {
+                pend_g = g;
+                pend_done = done;
+                std::lock_guard<std::mutex> lk(mu);
+                ++batches;
+                max_batch = std::max<int64_t>(max_batch, (int64_t)batch.size());
+                continue;  // the callback hands the jobs to the greedy pool
+            }
+            delete d;
+            ig_graph_free(g);
+        } else if (s == IG_OK) {
             s = ig::download_for_greedy(g, opts.order_threads, *hg);
             ig_graph_free(g);
         }
