@@ -221,16 +221,19 @@ def profile_traffic(wl_name):
 
 
 def alu_ops_per_pair(L: int, d: int) -> float:
-    """ALU-pipe operations (LOP3 + PRMT) the pair-test recurrence issues per
-    pair test, counted from the kernel source: the banded 8-lane form (two
-    rows x four columns) takes 9 per character step for 8 pairs plus 2 per
-    nibble-counter flush (every 7 steps and at the end) and 2 for the
-    threshold (editDist <= 4); the 4-lane form 9 per step for 4 pairs plus 1
-    (editDist 5..8); full Myers 8 per step for 2 pairs (L <= 15) or for 1."""
+    """ALU-pipe operations (LOP3, PRMT, the add and the shift) the pair-test
+    recurrence issues per pair test, counted from the kernel source (the lane
+    counter runs as an IMAD on the FMA pipe and is not counted).  Banded
+    8-lane form (two rows x four columns, editDist <= 4): 11 per character
+    step for 8 pairs, 5 fewer in the last step (its vertical deltas are not
+    needed), 3 per nibble-counter flush (every 7 steps and at the end) and 4
+    for the threshold.  4-lane form (editDist 5..8): 11 per step for 4 pairs,
+    5 fewer in the last step, 2 for the threshold.  Full Myers: 8 per step
+    for 2 pairs (L <= 15) or for 1."""
     if 1 <= d <= 4:
-        return (9.0 * L + 2 * -(-L // 7) + 2) / 8
+        return (11.0 * L - 5 + 3 * -(-L // 7) + 4) / 8
     if 5 <= d <= 8:
-        return (9.0 * L + 1) / 4
+        return (11.0 * L - 5 + 2) / 4
     return 8.0 / 2 * L if L <= 15 else 8.0 * L
 
 
@@ -595,7 +598,7 @@ def run_ours(args, wl, rank, world, dist):
         "roofline": {"bound": "int32-alu-pipe", "achieved": achieved, "peak": alu_peak, "unit": "Tops/s",
                      "frac": (achieved / alu_peak) if achieved else None, "traffic": traffic,
                      "kernel": "pair_kernel", "kernel_ms_per_launch": pair_avg_s * 1e3,
-                     "work": f"{pairs} pair tests x {alu_ops_per_pair(L, d):g} ALU-pipe ops (LOP3/PRMT) per pair "
+                     "work": f"{pairs} pair tests x {alu_ops_per_pair(L, d):g} ALU-pipe ops (LOP3/PRMT/add/shift) per pair "
                              f"test per launch",
                      "peak_source": f"{props.multi_processor_count} SMs x 64 ALU-pipe lanes/clk x {sm_mhz:.0f} MHz "
                                     f"max SM clock ({src} MEASURED_PEAKS sm_max_mhz)",

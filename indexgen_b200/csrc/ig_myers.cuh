@@ -195,9 +195,12 @@ __device__ __forceinline__ int myers_one_dist(uint32_t p01, uint32_t p23, const 
 // bit; D0 is masked to the band before it is shifted.  Y is not masked: its
 // spare bit may hold the next lane's bit 0, which reaches VN's spare bit only
 // (HP's spare bit is always 1, so VP's stays 0) and is masked out of D0.
-// Per character step kNib issues 9 ALU-pipe ops (1 PRMT + 8 LOP3) and 3
-// FMA-pipe ops (IMAD / IMAD.HI) for eight pair tests (two rows x four
-// columns), kByte 9 ALU + 3.5 FMA for four (one row x four columns).  The
+// Per character step kNib issues 11 ALU-pipe ops (1 PRMT, 8 LOP3, the add,
+// the shift) and one IMAD (the lane counter, off the critical path) for eight
+// pair tests (two rows x four columns), kByte the same for four (one row x
+// four columns).  (Moving the add and the shift to the FMA pipe as IMAD /
+// IMAD.HI, as an earlier form did, cut the ALU count to 9 but ran 7 % slower:
+// IMAD.HI is half rate and both sit on the recurrence's critical path.)  The
 // match masks of all lanes come from one PRMT on a window register W_j whose
 // byte c is the band window of Peq[c] at column j (kNib: two rows' windows,
 // one per nibble).  Lane counters of the centre bits (weight 2^w per byte)
@@ -265,22 +268,22 @@ __device__ __forceinline__ void band_nib2(const uint32_t (&W2)[L], const uint32_
 #pragma unroll
     for (int j = 0; j < L; ++j) {
         const uint32_t eq = __byte_perm(W2[j], W2[j], sel[j]);
-        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t sum = (eq & vp) + vp;
         const uint32_t d0 = ((sum ^ vp) | eq | vn) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
-        acc = imad(d0 & q.c, q.one, acc);
+        acc = imad(d0 & q.c, q.one, acc);  // off the critical path: on the FMA pipe
         if ((j + 1) % 7 == 0 || j == L - 1) {  // nibble counters hold at most 7 steps of 2^w
             be = imad(acc & 0x0f0f0f0fu, q.one, be);
-            bo = imad(__umulhi(acc, q.h28) & 0x0f0f0f0fu, q.one, bo);
+            bo = imad((acc >> 4) & 0x0f0f0f0fu, q.one, bo);
             acc = 0u;
         }
-        const uint32_t ys = __umulhi(d0, q.h31);  // spare bits may pick up a neighbour's bit 0
+        const uint32_t ys = d0 >> 1;  // spare bits may pick up a neighbour's bit 0
         vn = ys & hp;
         vp = hn | ~(ys | hp);
     }
-    he = imad(be, q.one, q.k) & 0x80808080u;
-    ho = imad(bo, q.one, q.k) & 0x80808080u;
+    he = (be + q.k) & 0x80808080u;
+    ho = (bo + q.k) & 0x80808080u;
 }
 
 // Four pair tests (one row, four columns); hit flag of column l at bit 8l+7.
@@ -292,12 +295,12 @@ __device__ __forceinline__ uint32_t band_byte(const uint32_t (&W)[L], const uint
     for (int j = 0; j < L; ++j) {
         const uint32_t s = (j & 1) ? __umulhi(sel[j >> 1], q.h16) : sel[j >> 1];
         const uint32_t eq = __byte_perm(W[j], W[j], s);
-        const uint32_t sum = imad(eq & vp, q.one, vp);
+        const uint32_t sum = (eq & vp) + vp;
         const uint32_t d0 = ((sum ^ vp) | eq | vn) & q.bm;
         const uint32_t hn = vp & d0;
         const uint32_t hp = vn | ~(d0 | vp);
-        acc = imad(d0 & q.c, q.one, acc);
-        const uint32_t ys = __umulhi(d0, q.h31);
+        acc = imad(d0 & q.c, q.one, acc);  // off the critical path: on the FMA pipe
+        const uint32_t ys = d0 >> 1;
         vn = ys & hp;
         vp = hn | ~(ys | hp);
     }
