@@ -220,11 +220,9 @@ struct PairArgs {
     const JobDesc *jobs;
     int njobs;
     long long items;
-    uint32_t one;     // 1, 2, 2^16, 2^28, 2^31 as opaque operands for imad / umulhi
+    uint32_t one;     // 1, 2, 2^16 as opaque operands for imad / umulhi
     uint32_t two;
     uint32_t hi;
-    uint32_t h28;
-    uint32_t h31;
     uint32_t gather;  // 0x00204081 and 16, opaque: hit flags -> column mask on the FMA pipe
     uint32_t h4;
     unsigned long long *work;
@@ -503,8 +501,6 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
         q.k = J.kthr;
         q.one = a.one;
         q.h16 = a.hi;
-        q.h28 = a.h28;
-        q.h31 = a.h31;
     }
     // c_lo is a multiple of 256 (segments and bands are), so units never
     // straddle a segment
@@ -825,8 +821,6 @@ __device__ __forceinline__ void run_item_nib(const PairArgs &a, const JobDesc &J
     q.k = J.kthr;
     q.one = a.one;
     q.h16 = a.hi;
-    q.h28 = a.h28;
-    q.h31 = a.h31;
     const int32_t c_lo = (int32_t)max((long long)seg << J.seg_shift, (long long)row0);
     const int32_t c_hi = (int32_t)min((long long)(seg + 1) << J.seg_shift, (long long)J.n);
     const long long row_end = (long long)row0 + kBandRows;
@@ -1358,8 +1352,6 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
     a.one = 1u;
     a.two = 2u;
     a.hi = 1u << 16;
-    a.h28 = 1u << 28;
-    a.h31 = 1u << 31;
     a.gather = 0x00204081u;
     a.h4 = 16u;
     a.work = flags + 0;

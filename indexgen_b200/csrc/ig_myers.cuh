@@ -251,7 +251,7 @@ __device__ __forceinline__ void band_windows(uint32_t word, int w, uint32_t (&W)
 
 struct BandConst {
     uint32_t vp0, bm, c, k;       // initial VP, band mask, centre mask, threshold constant
-    uint32_t one, h16, h28, h31;  // opaque 1, 2^16, 2^28, 2^31 (IMAD / IMAD.HI operands)
+    uint32_t one, h16;            // opaque 1 and 2^16 (IMAD / IMAD.HI operands)
 };
 
 // Eight pair tests: two rows A, B of one thread against four columns.  W2[j]
