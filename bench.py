@@ -273,18 +273,17 @@ def run_batch_section(ctx, reps: int = 3) -> dict:
     pairs = sum(len(w) * (len(w) - 1) // 2 for w in parts)
     cores = host_cores()
     books, edges = solve_batch(jobs, host_threads=cores, ctx=ctx)  # warm-up (workspace growth)
-    t_batch = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        books, edges = solve_batch(jobs, host_threads=cores, ctx=ctx)
-        t_batch.append(time.perf_counter() - t0)
-    # the same batch with direct launches instead of the captured CUDA graphs
-    ctx.set_graphs(False)
-    t_direct = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        solve_batch(jobs, host_threads=cores, ctx=ctx)
-        t_direct.append(time.perf_counter() - t0)
+    # captured CUDA graphs (the default) and direct launches, alternated so
+    # that neither side gets the warmer host
+    t_batch, t_direct = [], []
+    for _ in range(reps + 1):
+        for graphs, out in ((True, t_batch), (False, t_direct)):
+            ctx.set_graphs(graphs)
+            t0 = time.perf_counter()
+            b, e = solve_batch(jobs, host_threads=cores, ctx=ctx)
+            out.append(time.perf_counter() - t0)
+            if graphs:
+                books, edges = b, e
     ctx.set_graphs(True)
     # one more pass with per-phase events (they add syncs, so it is not timed)
     ctx.set_profiling(True)
