@@ -67,3 +67,18 @@ def test_replica_rate():
     assert bench.replica_rate(1, 10**9, 1, 1.0) == 1.0
     assert bench.replica_rate(4, 10**9, 3, 2.0) == 6.0
     assert bench.max_over_ranks(3.5, None, "cpu") == 3.5
+
+
+def test_alu_op_counts():
+    """The roofline's ALU-pipe op counts per pair test, per lane form, as
+    derived from the recurrences in ig_myers.cuh (11 ALU ops per character
+    step; 5 fewer in the last step; flushes and threshold)."""
+    import sys
+
+    sys.path.insert(0, ROOT)
+    import bench
+
+    assert bench.alu_ops_per_pair(12, 4) == (11 * 12 - 5 + 3 * 2 + 4) / 8 == 17.125
+    assert bench.alu_ops_per_pair(7, 3) == (11 * 7 - 5 + 3 * 1 + 4) / 8
+    assert bench.alu_ops_per_pair(16, 5) == (11 * 16 - 3) / 4 == 43.25
+    assert bench.alu_ops_per_pair(12, 9) == 4 * 12 and bench.alu_ops_per_pair(16, 9) == 8 * 16
