@@ -590,6 +590,7 @@ const char *ig_status_string(ig_status s)
 
 ig_status ig_ctx_create(ig_ctx **out, int device)
 {
+    IG_ABI_TRY
     if (!out)
         return IG_ERR_INPUT;
     *out = nullptr;
@@ -621,10 +622,12 @@ ig_status ig_ctx_create(ig_ctx **out, int device)
     cudaGetLastError();
     *out = c;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_destroy(ig_ctx *ctx)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     {
@@ -652,22 +655,26 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
     }
     delete ctx;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 const char *ig_last_error(const ig_ctx *ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
 ig_status ig_ctx_stream(ig_ctx *ctx, void **stream)
 {
+    IG_ABI_TRY
     if (!ctx || !stream)
         return IG_ERR_INPUT;
     *stream = (void *)ctx->stream;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 int64_t ig_ctx_launches(const ig_ctx *ctx) { return ctx ? ctx->launches : -1; }
 
 ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -684,10 +691,12 @@ ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable)
         ctx->phase_pending[p] = false;
     }
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches)
 {
+    IG_ABI_TRY
     if (!ctx || phase < 0 || phase > 2)
         return IG_ERR_INPUT;
     if (ms)
@@ -695,10 +704,12 @@ ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *l
     if (launches)
         *launches = ctx->phase_launches[phase];
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges)
 {
+    IG_ABI_TRY
     if (!ctx || edges < 0)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -717,11 +728,13 @@ ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges)
     ctx->records.bytes = bytes;
     ctx->rec_capacity = (unsigned long long)edges;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
                          ig_graph **out)
 {
+    IG_ABI_TRY
     if (!ctx || !out)
         return IG_ERR_INPUT;
     *out = nullptr;
@@ -744,18 +757,22 @@ ig_status ig_graph_build(ig_ctx *ctx, const uint32_t *words, int32_t n, int len,
     }
     *out = g;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_free(ig_graph *g)
 {
+    IG_ABI_TRY
     if (!g)
         return IG_ERR_INPUT;
     ig::release_graph(g);
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_stats(const ig_graph *g, int32_t *n, int64_t *edges)
 {
+    IG_ABI_TRY
     if (!g)
         return IG_ERR_INPUT;
     if (n)
@@ -763,10 +780,12 @@ ig_status ig_graph_stats(const ig_graph *g, int32_t *n, int64_t *edges)
     if (edges)
         *edges = g->edges;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_upper_csr(const ig_graph *g, int64_t *row_ptr, int32_t *cols)
 {
+    IG_ABI_TRY
     if (!g || !row_ptr || (g->edges > 0 && !cols))
         return IG_ERR_INPUT;
     ig::Ctx *ctx = g->ctx;
@@ -789,10 +808,12 @@ ig_status ig_graph_upper_csr(const ig_graph *g, int64_t *row_ptr, int32_t *cols)
     if (e != cudaSuccess)
         return ig::cuda_error(ctx, e, "CSR download");
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_pairs(const ig_graph *gc, int32_t *pairs)
 {
+    IG_ABI_TRY
     ig_graph *g = const_cast<ig_graph *>(gc);
     if (!g || (g->edges > 0 && !pairs))
         return IG_ERR_INPUT;
@@ -807,19 +828,23 @@ ig_status ig_graph_pairs(const ig_graph *gc, int32_t *pairs)
             ++k;
         }
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_device_csr(const ig_graph *g, const int64_t **row_ptr, const int32_t **cols)
 {
+    IG_ABI_TRY
     if (!g || !row_ptr || !cols)
         return IG_ERR_INPUT;
     *row_ptr = g->d_row_ptr;
     *cols = g->d_cols;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_adjacency(ig_graph *g, int64_t *adj_ptr, int32_t *adj)
 {
+    IG_ABI_TRY
     if (!g || !adj_ptr || (g->edges > 0 && !adj))
         return IG_ERR_INPUT;
     ig::Ctx *ctx = g->ctx;
@@ -838,10 +863,12 @@ ig_status ig_graph_adjacency(ig_graph *g, int64_t *adj_ptr, int32_t *adj)
     if (e != cudaSuccess)
         return ig::cuda_error(ctx, e, "adjacency download");
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_device_adjacency(ig_graph *g, const int64_t **adj_ptr, const int32_t **adj)
 {
+    IG_ABI_TRY
     if (!g || !adj_ptr || !adj)
         return IG_ERR_INPUT;
     ig::Ctx *ctx = g->ctx;
@@ -853,10 +880,12 @@ ig_status ig_graph_device_adjacency(ig_graph *g, const int64_t **adj_ptr, const 
     *adj_ptr = g->d_adj_ptr;
     *adj = g->d_adj;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int32_t *count)
 {
+    IG_ABI_TRY
     if (!g || !count || order_threads < 1 || (g->n > 0 && !order))
         return IG_ERR_INPUT;
     if (g->jobs.size() != 1)
@@ -866,18 +895,22 @@ ig_status ig_graph_codebook(ig_graph *g, int order_threads, int32_t *order, int3
     if (s == IG_OK)
         *count = c;
     return s;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_job_count(const ig_graph *g, int32_t *jobs)
 {
+    IG_ABI_TRY
     if (!g || !jobs)
         return IG_ERR_INPUT;
     *jobs = (int32_t)g->jobs.size();
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word, int32_t *n, int64_t *edges)
 {
+    IG_ABI_TRY
     if (!g || job < 0 || job >= (int32_t)g->jobs.size())
         return IG_ERR_INPUT;
     if (first_word)
@@ -887,18 +920,22 @@ ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word
     if (edges)
         *edges = g->job_edge_off[(size_t)job + 1] - g->job_edge_off[(size_t)job];
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_job_codebooks(ig_graph *g, int order_threads, int host_threads, int32_t *order, int32_t *counts)
 {
+    IG_ABI_TRY
     if (!g || order_threads < 1 || (g->n > 0 && !order) || (!g->jobs.empty() && !counts))
         return IG_ERR_INPUT;
     return ig::job_codebooks_impl(g, order_threads, host_threads, order, counts);
+    IG_ABI_CATCH
 }
 
 ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
                          const int32_t *lens, const int32_t *min_eds, int words_on_device, ig_graph **out)
 {
+    IG_ABI_TRY
     if (!ctx || !out)
         return IG_ERR_INPUT;
     *out = nullptr;
@@ -926,12 +963,14 @@ ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     }
     *out = g;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
                          const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
                          int32_t *order, int32_t *counts, int64_t *edges)
 {
+    IG_ABI_TRY
     if (!ctx || order_threads < 1 || (jobs > 0 && (!order || !counts)))
         return IG_ERR_INPUT;
     std::vector<ig::JobSpec> spec;
@@ -940,10 +979,12 @@ ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
         return s;
     return ig::solve_groups(ctx, words, 0, offsets, jobs, lens, min_eds, order_threads, host_threads, order, counts,
                             edges);
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_write_adj_list(ig_graph *g, const char *path, int64_t *bytes)
 {
+    IG_ABI_TRY
     if (!g || !path)
         return IG_ERR_INPUT;
     ig::Ctx *ctx = g->ctx;
@@ -952,10 +993,12 @@ ig_status ig_graph_write_adj_list(ig_graph *g, const char *path, int64_t *bytes)
     if (!dg.ok)
         return ig::set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
     return ig::write_adj_list(ctx, g, path, bytes);
+    IG_ABI_CATCH
 }
 
 ig_status ig_graph_read_adj_list(ig_ctx *ctx, const char *path, ig_graph **out)
 {
+    IG_ABI_TRY
     if (!ctx || !path || !out)
         return IG_ERR_INPUT;
     *out = nullptr;
@@ -973,11 +1016,13 @@ ig_status ig_graph_read_adj_list(ig_ctx *ctx, const char *path, ig_graph **out)
     }
     *out = g;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const uint32_t *centers, int32_t k,
                             int len, int on_device, int32_t *assignment)
 {
+    IG_ABI_TRY
     if (!ctx || n < 0 || k < 0 || len < 1 || len > IG_MAX_LEN)
         return IG_ERR_INPUT;
     if (n == 0)
@@ -1018,11 +1063,13 @@ ig_status ig_assign_centers(ig_ctx *ctx, const uint32_t *words, int64_t n, const
     if (e == cudaSuccess)
         e = cudaStreamSynchronize(st);
     return e == cudaSuccess ? IG_OK : ig::cuda_error(ctx, e, "assignment download");
+    IG_ABI_CATCH
 }
 
 ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,
                    int32_t *order, int32_t *count, int64_t *edges)
 {
+    IG_ABI_TRY
     if (!ctx || !count || order_threads < 1 || (n > 0 && !order))
         return IG_ERR_INPUT;
     ig_graph *g = nullptr;
@@ -1034,10 +1081,12 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
     s = ig_graph_codebook(g, order_threads, order, count);
     ig::release_graph(g);
     return s;
+    IG_ABI_CATCH
 }
 
 ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *edges)
 {
+    IG_ABI_TRY
     if (!ctx || !edges)
         return IG_ERR_INPUT;
     if (ig::check_job(words, n, len) != IG_OK)
@@ -1049,6 +1098,7 @@ ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int 
     if (s != IG_OK)
         return s;
     return ig::count_batch(ctx, d_words, {ig::JobSpec{0, n, len, min_ed}}, edges);
+    IG_ABI_CATCH
 }
 
 int ig_lane_form(int len, int min_ed)
@@ -1061,6 +1111,7 @@ int ig_lane_form(int len, int min_ed)
 ig_status ig_ctx_autotune(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int words_on_device,
                           int32_t *items_per_cta)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     if (ig::check_job(words, n, len) != IG_OK || n < 2 || min_ed < 1)
@@ -1077,20 +1128,24 @@ ig_status ig_ctx_autotune(ig_ctx *ctx, const uint32_t *words, int32_t n, int len
     if (s == IG_OK && items_per_cta)
         *items_per_cta = chosen;
     return s;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_cta)
 {
+    IG_ABI_TRY
     if (!ctx || lane_form < 0 || lane_form > 2 || items_per_cta < 1 || items_per_cta > 4096)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->items_per_cta[lane_form] = items_per_cta;
     ctx->tuned[lane_form] = true;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned)
 {
+    IG_ABI_TRY
     if (!ctx || lane_form < 0 || lane_form > 2)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
@@ -1099,19 +1154,23 @@ ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, 
     if (tuned)
         *tuned = ctx->tuned[lane_form] ? 1 : 0;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_set_graphs(ig_ctx *ctx, int enable)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->use_graphs = enable != 0;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *instantiations, int64_t *updates)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     if (launches)
@@ -1121,15 +1180,18 @@ ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *inst
     if (updates)
         *updates = ctx->graph_updates;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable)
 {
+    IG_ABI_TRY
     if (!ctx)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->autotune = enable != 0;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 }  // extern "C"

@@ -82,6 +82,7 @@ extern "C" ig_status ig_cluster_solve(ig_ctx *ctx, const uint32_t *words, int32_
                                       int32_t converge_iters, uint64_t seed, int32_t max_iters, int host_threads,
                                       int32_t *codebook, int32_t *count, int32_t *iterations, int64_t *sizes)
 {
+    IG_ABI_TRY
     using namespace ig;
     if (!ctx || n < 0 || len < 1 || len > IG_MAX_LEN || max_iters < 1 || !count || (n > 0 && (!words || !codebook)))
         return IG_ERR_INPUT;
@@ -216,4 +217,5 @@ extern "C" ig_status ig_cluster_solve(ig_ctx *ctx, const uint32_t *words, int32_
     if (iterations)
         *iterations = iteration;
     return IG_OK;
+    IG_ABI_CATCH
 }

@@ -273,6 +273,7 @@ extern "C" {
 
 ig_status ig_pack(const char *text, int64_t n, int len, int64_t stride, uint32_t *out, int64_t *bad_row)
 {
+    IG_ABI_TRY
     if (n < 0 || len < 1 || len > IG_MAX_LEN || stride < len || (n > 0 && (!text || !out)))
         return IG_ERR_INPUT;
     for (int64_t i = 0; i < n; ++i) {
@@ -292,11 +293,13 @@ ig_status ig_pack(const char *text, int64_t n, int len, int64_t stride, uint32_t
     if (bad_row)
         *bad_row = -1;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_filter(const uint32_t *words, int64_t n, int len, int max_run, double min_gc, double max_gc,
                     uint8_t *keep)
 {
+    IG_ABI_TRY
     if (n < 0 || len < 1 || len > IG_MAX_LEN || (n > 0 && (!words || !keep)))
         return IG_ERR_INPUT;
     const bool use_run = max_run > 0;
@@ -329,11 +332,13 @@ ig_status ig_filter(const uint32_t *words, int64_t n, int len, int max_run, doub
         keep[i] = ok ? 1 : 0;
     }
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count)
 {
+    IG_ABI_TRY
     if (n < 0 || !count || (n > 0 && (!row_ptr || !order)) || (n > 0 && row_ptr[n] > 0 && !cols))
         return IG_ERR_INPUT;
     if (order_threads < 1)
@@ -350,6 +355,7 @@ ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols
         return IG_ERR_OOM;
     }
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 }  // extern "C"

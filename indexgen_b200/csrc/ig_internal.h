@@ -11,9 +11,26 @@
 #include <string>
 #include <vector>
 
+#include <new>
+
 #include <cuda_runtime.h>
 
 #include "indexgen_cuda.h"
+
+// Every ig_status entry point runs its body between IG_ABI_TRY and
+// IG_ABI_CATCH, so no C++ exception crosses the C ABI: an allocation failure
+// in host code becomes IG_ERR_OOM, anything else IG_ERR_STATE.
+#define IG_ABI_TRY try {
+#define IG_ABI_CATCH                        \
+    }                                       \
+    catch (const std::bad_alloc &)          \
+    {                                       \
+        return IG_ERR_OOM;                  \
+    }                                       \
+    catch (...)                             \
+    {                                       \
+        return IG_ERR_STATE;                \
+    }
 
 namespace ig {
 

@@ -151,6 +151,7 @@ void *g_addr[256] = {};
 extern "C" ig_status ig_count_conflicts_noalloc(const uint32_t *words, int32_t n, int len, int min_ed,
                                                 unsigned long long *count, void *stream)
 {
+    IG_ABI_TRY
     using namespace ig;
     if (!count || len < 1 || len > IG_MAX_LEN || n < 0 || (n > 0 && !words))
         return IG_ERR_INPUT;
@@ -195,4 +196,5 @@ extern "C" ig_status ig_count_conflicts_noalloc(const uint32_t *words, int32_t n
         return IG_ERR_CUDA;
     }
     return IG_OK;
+    IG_ABI_CATCH
 }

@@ -266,6 +266,7 @@ extern "C" {
 
 ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **out)
 {
+    IG_ABI_TRY
     if (!ctx || !out)
         return IG_ERR_INPUT;
     *out = nullptr;
@@ -310,10 +311,12 @@ ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **
         sv->pool.emplace_back([sv] { sv->greedy_loop(); });
     *out = sv;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_submit(ig_server *sv, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *ticket)
 {
+    IG_ABI_TRY
     if (!sv || !ticket || n < 0 || len < 1 || len > IG_MAX_LEN || (n > 0 && !words))
         return IG_ERR_INPUT;
     auto j = std::make_shared<ServerJob>();
@@ -337,10 +340,12 @@ ig_status ig_server_submit(ig_server *sv, const uint32_t *words, int32_t n, int 
     *ticket = j->ticket;
     sv->cv_queue.notify_one();
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_poll(ig_server *sv, int64_t ticket, int *state)
 {
+    IG_ABI_TRY
     if (!sv || !state)
         return IG_ERR_INPUT;
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -349,11 +354,13 @@ ig_status ig_server_poll(ig_server *sv, int64_t ticket, int *state)
         return IG_ERR_INPUT;
     *state = (int)it->second->state;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_wait(ig_server *sv, int64_t ticket, int32_t *order, int32_t *count, int64_t *edges,
                          double *latency_ms)
 {
+    IG_ABI_TRY
     if (!sv || !count)
         return IG_ERR_INPUT;
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -377,10 +384,12 @@ ig_status ig_server_wait(ig_server *sv, int64_t ticket, int32_t *order, int32_t 
     if (edges)
         *edges = j->edges;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_cancel(ig_server *sv, int64_t ticket)
 {
+    IG_ABI_TRY
     if (!sv)
         return IG_ERR_INPUT;
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -394,10 +403,12 @@ ig_status ig_server_cancel(ig_server *sv, int64_t ticket)
     ++sv->cancelled;
     sv->cv_done.notify_all();
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, int64_t *max_batch_jobs)
 {
+    IG_ABI_TRY
     if (!sv)
         return IG_ERR_INPUT;
     std::unique_lock<std::mutex> lk(sv->mu);
@@ -408,10 +419,12 @@ ig_status ig_server_stats(ig_server *sv, int64_t *batches, int64_t *completed, i
     if (max_batch_jobs)
         *max_batch_jobs = sv->max_batch;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 ig_status ig_server_destroy(ig_server *sv)
 {
+    IG_ABI_TRY
     if (!sv)
         return IG_ERR_INPUT;
     {
@@ -438,6 +451,7 @@ ig_status ig_server_destroy(ig_server *sv)
         t.join();
     delete sv;
     return IG_OK;
+    IG_ABI_CATCH
 }
 
 }  // extern "C"
