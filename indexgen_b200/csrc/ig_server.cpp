@@ -306,9 +306,14 @@ ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **
     if (o.pool_reserve_bytes > 0)
         ig::reserve_pool(ctx, (size_t)o.pool_reserve_bytes);  // best effort
     sv->opts = o;
-    sv->scheduler = std::thread([sv] { sv->schedule_loop(); });
-    for (int i = 0; i < o.host_threads; ++i)
-        sv->pool.emplace_back([sv] { sv->greedy_loop(); });
+    try {
+        sv->scheduler = std::thread([sv] { sv->schedule_loop(); });
+        for (int i = 0; i < o.host_threads; ++i)
+            sv->pool.emplace_back([sv] { sv->greedy_loop(); });
+    } catch (...) {  // a thread could not start: stop the ones that did
+        ig_server_destroy(sv);
+        return IG_ERR_OOM;
+    }
     *out = sv;
     return IG_OK;
     IG_ABI_CATCH
