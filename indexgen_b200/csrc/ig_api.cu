@@ -378,7 +378,8 @@ GreedyPool::~GreedyPool()
         th.join();
 }
 
-void GreedyPool::submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts)
+void GreedyPool::submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts,
+                        const std::shared_ptr<Ticket> &ticket)
 {
     {
         std::lock_guard<std::mutex> lk(mu_);
@@ -390,28 +391,33 @@ void GreedyPool::submit(std::shared_ptr<const HostGraph> hg, int64_t order_base,
             t.job = j;
             t.out = order + (hg->jobs[(size_t)j].word_off - order_base);
             t.count = counts + j;
+            t.ticket = ticket;
+            ticket->left++;
             q_.push(std::move(t));
         }
     }
     cv_.notify_all();
 }
 
-bool GreedyPool::wait()
+bool GreedyPool::wait(const std::shared_ptr<Ticket> &ticket)
 {
     // the waiting thread is done driving the device: it runs queued
-    // greedies too, then waits for the ones in flight
+    // greedies too (the largest first, whoever queued them) until its own
+    // jobs have finished
     std::unique_lock<std::mutex> lk(mu_);
-    while (!q_.empty())
-        run_one(lk);
-    idle_.wait(lk, [this]() { return q_.empty() && busy_ == 0; });
-    return !failed_;
+    while (ticket->left > 0) {
+        if (!q_.empty())
+            run_one(lk);
+        else
+            done_.wait(lk);
+    }
+    return !ticket->failed;
 }
 
 void GreedyPool::run_one(std::unique_lock<std::mutex> &lk)
 {
     Task t = q_.top();
     q_.pop();
-    ++busy_;
     lk.unlock();
     bool ok = true;
     try {
@@ -421,11 +427,10 @@ void GreedyPool::run_one(std::unique_lock<std::mutex> &lk)
     }
     t.hg.reset();  // the last task of a graph frees its host copy here
     lk.lock();
-    --busy_;
     if (!ok)
-        failed_ = true;
-    if (q_.empty() && busy_ == 0)
-        idle_.notify_all();
+        t.ticket->failed = true;
+    if (--t.ticket->left == 0)
+        done_.notify_all();
 }
 
 void GreedyPool::work()
@@ -439,16 +444,27 @@ void GreedyPool::work()
     }
 }
 
+std::shared_ptr<GreedyPool> shared_greedy_pool(Ctx *ctx)
+{
+    std::lock_guard<std::mutex> lk(ctx->greedy_mu);
+    if (!ctx->greedy_pool) {
+        const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+        ctx->greedy_pool = std::make_shared<GreedyPool>(std::max(1, hw - 1));
+    }
+    return ctx->greedy_pool;
+}
+
 // Host callback of a group's adjacency copy: queues the group's greedies.
 struct SubmitWhenCopied {
     GreedyPool *pool;
     std::shared_ptr<HostGraph> hg;
     int32_t *order;
     int32_t *counts;
+    std::shared_ptr<GreedyPool::Ticket> ticket;
     static void CUDART_CB run(void *p)
     {
         std::unique_ptr<SubmitWhenCopied> c(static_cast<SubmitWhenCopied *>(p));
-        c->pool->submit(c->hg, 0, c->order, c->counts);
+        c->pool->submit(c->hg, 0, c->order, c->counts, c->ticket);
     }
 };
 
@@ -477,11 +493,19 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
     }
     cut.push_back(jobs);
     ig_status s = IG_OK;
-    // One core stays with this thread: it drives the device, and a build
-    // that waits for a core behind the greedies stalls the whole pipeline.
+    // The greedies run on the context's pool (one thread fewer than the
+    // cores: this thread drives the device, and a build that waits for a
+    // core behind the greedies stalls the whole pipeline), or on a pool of
+    // their own when the caller asks for fewer threads than that.
     const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
     const int cap = std::max(1, hw - 1);
-    GreedyPool pool(std::max(1, std::min({host_threads > 0 ? host_threads : cap, cap, (int)jobs})));
+    std::shared_ptr<GreedyPool> pool_ref;
+    if (host_threads > 0 && host_threads < cap)
+        pool_ref = std::make_shared<GreedyPool>(std::max(1, std::min<int>(host_threads, jobs)));
+    else
+        pool_ref = shared_greedy_pool(ctx);
+    GreedyPool &pool = *pool_ref;
+    const auto ticket = std::make_shared<GreedyPool::Ticket>();
     // A group whose adjacency copy runs on the download stream while the
     // next group builds; the copy's host callback queues its greedies the
     // moment it lands, and the group's device buffers are freed after the
@@ -527,7 +551,7 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
         auto hg = std::make_shared<HostGraph>();
         if (order_threads == 1) {
             cudaEvent_t done = nullptr;
-            auto *sub_ctx = new SubmitWhenCopied{&pool, hg, order + offsets[lo], counts + lo};
+            auto *sub_ctx = new SubmitWhenCopied{&pool, hg, order + offsets[lo], counts + lo, ticket};
             s = fetch_adjacency_async(g, *hg, &done, SubmitWhenCopied::run, sub_ctx);
             if (s != IG_OK) {
                 delete sub_ctx;
@@ -541,13 +565,13 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
             release_graph(g);
             if (s != IG_OK)
                 break;
-            pool.submit(hg, 0, order + offsets[lo], counts + lo);
+            pool.submit(hg, 0, order + offsets[lo], counts + lo, ticket);
         }
     }
     const ig_status f = finish();
     if (s == IG_OK)
         s = f;
-    const bool host_ok = pool.wait();
+    const bool host_ok = pool.wait(ticket);
     if (s == IG_OK && !host_ok)
         s = set_error(ctx, IG_ERR_OOM, "host greedy allocation failed");
     return s;
@@ -642,6 +666,7 @@ ig_status ig_ctx_destroy(ig_ctx *ctx)
         for (cudaEvent_t e : ctx->ev)
             if (e)
                 cudaEventDestroy(e);
+        ctx->greedy_pool.reset();  // joins its threads (no call is running on a context being destroyed)
         for (cudaGraphExec_t x : ctx->graph_exec)
             if (x)
                 cudaGraphExecDestroy(x);

@@ -129,6 +129,9 @@ struct Ctx {
     int64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
     // second stream for device-to-host copies that overlap the next build
     cudaStream_t dl_stream = nullptr;
+    // host threads for batch greedies, shared by the calls on this context
+    std::mutex greedy_mu;
+    std::shared_ptr<class GreedyPool> greedy_pool;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
     size_t stage_bytes = 0;
@@ -250,14 +253,20 @@ ig_status solve_groups(ig_ctx *ctx, const uint32_t *words, int words_on_device, 
 // idle threads take jobs of any group (ig_api.cu).
 class GreedyPool {
   public:
+    // One caller's jobs: how many are unfinished, and whether one failed.
+    struct Ticket {
+        int left = 0;
+        bool failed = false;
+    };
     explicit GreedyPool(int threads);
-    ~GreedyPool();  // waits for the queued jobs
-    // Queues every job of hg: job j's selection goes to order + word_off_j -
-    // order_base, its size to counts[j].
-    void submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts);
-    // Runs queued greedies on the calling thread too until the queue is
-    // empty, then waits for the rest; false if a greedy failed to allocate.
-    bool wait();
+    ~GreedyPool();  // callers have waited for their tickets
+    // Queues every job of hg under `ticket`: job j's selection goes to
+    // order + word_off_j - order_base, its size to counts[j].
+    void submit(std::shared_ptr<const HostGraph> hg, int64_t order_base, int32_t *order, int32_t *counts,
+                const std::shared_ptr<Ticket> &ticket);
+    // Runs queued greedies on the calling thread too until every job of
+    // `ticket` has finished; false if one of them failed to allocate.
+    bool wait(const std::shared_ptr<Ticket> &ticket);
 
   private:
     struct Task {
@@ -267,18 +276,21 @@ class GreedyPool {
         int job;
         int32_t *out;
         int32_t *count;
+        std::shared_ptr<Ticket> ticket;
         bool operator<(const Task &o) const { return edges != o.edges ? edges < o.edges : seq > o.seq; }
     };
     void work();
     void run_one(std::unique_lock<std::mutex> &lk);  // pops the top task; lk held on entry and exit
     std::mutex mu_;
-    std::condition_variable cv_, idle_;
+    std::condition_variable cv_, done_;
     std::priority_queue<Task> q_;
     std::vector<std::thread> threads_;
     int64_t seq_ = 0;
-    int busy_ = 0;
-    bool stop_ = false, failed_ = false;
+    bool stop_ = false;
 };
+
+// The context's greedy pool (cores - 1 threads), started on first use.
+std::shared_ptr<GreedyPool> shared_greedy_pool(Ctx *ctx);
 
 // Makes a device current for the duration of a call and restores the
 // caller's device afterwards.
