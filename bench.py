@@ -260,7 +260,7 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def run_batch_section(ctx, reps: int = 3) -> dict:
+def run_batch_section(ctx, reps: int = 6) -> dict:
     """Batched clusters (1,000,000 filtered uniform n=14 words, 64 clusters with
     Zipf(1.1) sizes in [2k, 60k], editDist 4): the whole batch as one device
     pipeline + per-cluster greedies on all host cores, against the plain path
