@@ -296,6 +296,40 @@ def run_batch_section(ctx, reps: int = 6) -> dict:
     for w, L, d in jobs:
         plain_books.append(solve(w, L, d, 1, ctx)[0])
     t_plain = time.perf_counter() - t0
+
+    # the reference host's pattern: a pool of worker threads, each calling
+    # solve() per cluster on one shared context (concurrent calls coalesced
+    # into batches by the library, then without that)
+    def threaded(coalesce: bool) -> float:
+        import threading
+
+        ctx.set_coalescing(coalesce)
+        nxt = iter(range(len(jobs)))
+        lock = threading.Lock()
+        out = [None] * len(jobs)
+
+        def worker():
+            while True:
+                with lock:
+                    j = next(nxt, None)
+                if j is None:
+                    return
+                w, L, d = jobs[j]
+                out[j] = solve(w, L, d, 1, ctx)[0]
+
+        th = [threading.Thread(target=worker) for _ in range(cores)]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        dt = time.perf_counter() - t0
+        ctx.set_coalescing(True)
+        assert all(np.array_equal(a, b) for a, b in zip(out, plain_books))
+        return dt
+
+    t_thr = min(threaded(True) for _ in range(3))
+    t_thr_off = min(threaded(False) for _ in range(3))
     same = all(np.array_equal(a, b) for a, b in zip(books, plain_books))
     tb = min(t_batch)
     return {"workload": "clusters64_n14_d4 (1,000,000 uniform n=14 words, 64 Zipf(1.1) clusters in [2k,60k])",
@@ -306,6 +340,8 @@ def run_batch_section(ctx, reps: int = 6) -> dict:
             "work_split_items_per_cta": ctx.work_split(1)[0], "work_split_tuned": ctx.work_split(1)[1],
             "plain_jobs_per_s": len(jobs) / t_plain, "plain_s": t_plain,
             "speedup_vs_plain": t_plain / tb,
+            "threaded_solve_jobs_per_s": len(jobs) / t_thr,
+            "threaded_solve_uncoalesced_jobs_per_s": len(jobs) / t_thr_off,
             "batched_pair_kernel_gpairs_per_s": (pairs / (pair_ms / 1e3) / 1e9) if pair_ms else None,
             "host_threads": cores, "identical_to_plain": bool(same),
             "note": "wall clock through solve_batch vs a loop of solve (graph + greedy per cluster)"}

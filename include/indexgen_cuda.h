@@ -106,6 +106,10 @@ ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_ct
 ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned);
 /* Automatic tuning on (1, default) or off (0). */
 ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable);
+/* Concurrent ig_solve calls built together (1, default) or one by one (0),
+ * and how many batches and calls have gone through the combiner. */
+ig_status ig_ctx_set_coalescing(ig_ctx *ctx, int enable);
+ig_status ig_ctx_coalesce_stats(ig_ctx *ctx, int64_t *batches, int64_t *requests);
 
 /* ---- CUDA graphs of the batch pipeline ---------------------------------- */
 /* Each build (single job or batch) is one CUDA graph launch on the
@@ -288,7 +292,12 @@ ig_status ig_cluster_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int le
 /* ---- one-call conveniences --------------------------------------------- */
 
 /* SolveIndependentSet (src/SparseMat.cpp:784-851): graph + greedy.
- * edges may be null. */
+ * edges may be null.  With order_threads = 1, calls made on one context from
+ * several host threads at once (the reference's cluster worker pool,
+ * src/SparseMat.cpp:978-1010) are built together: a call that finds the
+ * device busy leaves its job waiting, and the next caller to get the device
+ * builds every waiting job as one batch; each caller then runs its own
+ * greedy.  A lone call is built at once.  Results are the same either way. */
 ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int order_threads,
                    int32_t *order, int32_t *count, int64_t *edges);
 /* Number of conflicting pairs only (VerifyDist's GPU branch passes when it is

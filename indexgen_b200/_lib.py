@@ -25,7 +25,7 @@ EXPORTS = (
     "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
     "ig_server_stats", "ig_server_destroy",
     "ig_lane_form", "ig_ctx_autotune", "ig_ctx_set_work_split", "ig_ctx_work_split", "ig_ctx_set_autotune",
-    "ig_ctx_set_graphs", "ig_ctx_graph_stats",
+    "ig_ctx_set_graphs", "ig_ctx_graph_stats", "ig_ctx_set_coalescing", "ig_ctx_coalesce_stats",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -108,6 +108,8 @@ def _declare(L):
         "ig_ctx_set_autotune": (_int, [_vp, _int]),
         "ig_ctx_set_graphs": (_int, [_vp, _int]),
         "ig_ctx_graph_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
+        "ig_ctx_set_coalescing": (_int, [_vp, _int]),
+        "ig_ctx_coalesce_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

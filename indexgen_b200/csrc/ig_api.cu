@@ -444,6 +444,77 @@ void GreedyPool::work()
     }
 }
 
+// Concurrent ig_solve calls on one context, built together.  The reference
+// host solves clusters from a pool of worker threads, each calling its GPU
+// path on its own (src/SparseMat.cpp:978-1010); here a call that finds the
+// device busy leaves its job in `pending`, and whichever waiting caller gets
+// the device next builds every pending job as one batch (one persistent
+// pair launch, block-diagonal graph).  Each caller then runs its own job's
+// greedy on its own thread.  Nothing waits for company: a lone call is built
+// at once.
+struct SolveRequest {
+    const uint32_t *words = nullptr;
+    int32_t n = 0;
+    int len = 1, min_ed = 0;
+    std::shared_ptr<HostGraph> hg;  // the batch's adjacency on the host
+    int job = -1;                   // this request's job in it
+    int64_t edges = 0;
+    ig_status status = IG_OK;
+    bool ready = false;
+};
+
+struct SolveCombiner {
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<SolveRequest *> pending;
+    bool building = false;
+    int64_t batches = 0, requests = 0;
+};
+
+std::shared_ptr<SolveCombiner> solve_combiner(Ctx *ctx)
+{
+    std::lock_guard<std::mutex> lk(ctx->greedy_mu);
+    if (!ctx->combiner)
+        ctx->combiner = std::make_shared<SolveCombiner>();
+    return ctx->combiner;
+}
+
+// Builds the requests as one batch and downloads its canonical adjacency.
+void build_requests(ig_ctx *ctx, const std::vector<SolveRequest *> &reqs)
+{
+    ig_status s = IG_OK;
+    try {
+        std::vector<uint32_t> words;
+        std::vector<int64_t> off{0};
+        std::vector<int32_t> lens, eds;
+        for (SolveRequest *r : reqs) {
+            words.insert(words.end(), r->words, r->words + r->n);
+            off.push_back(off.back() + r->n);
+            lens.push_back(r->len);
+            eds.push_back(r->min_ed);
+        }
+        ig_graph *g = nullptr;
+        s = ig_batch_build(ctx, words.data(), off.data(), (int32_t)reqs.size(), lens.data(), eds.data(), 0, &g);
+        if (s == IG_OK) {
+            auto hg = std::make_shared<HostGraph>();
+            s = download_for_greedy(g, 1, *hg);
+            if (s == IG_OK)
+                for (size_t j = 0; j < reqs.size(); ++j) {
+                    reqs[j]->hg = hg;
+                    reqs[j]->job = (int)j;
+                    reqs[j]->edges = g->job_edge_off[j + 1] - g->job_edge_off[j];
+                }
+            release_graph(g);
+        }
+    } catch (const std::bad_alloc &) {
+        s = IG_ERR_OOM;
+    } catch (...) {  // the waiting callers must hear back whatever happens
+        s = IG_ERR_STATE;
+    }
+    for (SolveRequest *r : reqs)
+        r->status = s;
+}
+
 std::shared_ptr<GreedyPool> shared_greedy_pool(Ctx *ctx)
 {
     std::lock_guard<std::mutex> lk(ctx->greedy_mu);
@@ -1097,6 +1168,44 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
     IG_ABI_TRY
     if (!ctx || !count || order_threads < 1 || (n > 0 && !order))
         return IG_ERR_INPUT;
+    if (ctx->coalesce && order_threads == 1) {
+        if (ig::check_job(words, n, len) != IG_OK)
+            return ig::set_error(ctx, IG_ERR_INPUT, "words must be non-null, n >= 0 and 1 <= len <= 16");
+        ig::SolveRequest req;
+        req.words = words;
+        req.n = n;
+        req.len = len;
+        req.min_ed = min_ed;
+        const auto C = ig::solve_combiner(ctx);
+        {
+            std::unique_lock<std::mutex> lk(C->mu);
+            C->pending.push_back(&req);
+            while (!req.ready) {
+                if (!C->building) {  // the device is free: build everything that waits
+                    C->building = true;
+                    std::vector<ig::SolveRequest *> batch;
+                    batch.swap(C->pending);
+                    lk.unlock();
+                    ig::build_requests(ctx, batch);
+                    lk.lock();
+                    for (ig::SolveRequest *r : batch)
+                        r->ready = true;
+                    C->building = false;
+                    C->batches++;
+                    C->requests += (int64_t)batch.size();
+                    C->cv.notify_all();
+                } else {
+                    C->cv.wait(lk);
+                }
+            }
+        }
+        if (req.status != IG_OK)
+            return req.status;
+        if (edges)
+            *edges = req.edges;
+        *count = ig::greedy_one(*req.hg, req.job, order);
+        return IG_OK;
+    }
     ig_graph *g = nullptr;
     ig_status s = ig_graph_build(ctx, words, n, len, min_ed, 0, &g);
     if (s != IG_OK)
@@ -1204,6 +1313,31 @@ ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *inst
         *instantiations = ctx->graph_instantiations;
     if (updates)
         *updates = ctx->graph_updates;
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_set_coalescing(ig_ctx *ctx, int enable)
+{
+    IG_ABI_TRY
+    if (!ctx)
+        return IG_ERR_INPUT;
+    ctx->coalesce = enable != 0;
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_coalesce_stats(ig_ctx *ctx, int64_t *batches, int64_t *requests)
+{
+    IG_ABI_TRY
+    if (!ctx)
+        return IG_ERR_INPUT;
+    const auto C = ig::solve_combiner(ctx);
+    std::lock_guard<std::mutex> lk(C->mu);
+    if (batches)
+        *batches = C->batches;
+    if (requests)
+        *requests = C->requests;
     return IG_OK;
     IG_ABI_CATCH
 }

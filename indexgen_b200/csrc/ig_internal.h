@@ -132,6 +132,9 @@ struct Ctx {
     // host threads for batch greedies, shared by the calls on this context
     std::mutex greedy_mu;
     std::shared_ptr<class GreedyPool> greedy_pool;
+    // concurrent ig_solve calls built together (ig_api.cu)
+    bool coalesce = true;
+    std::shared_ptr<struct SolveCombiner> combiner;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
     size_t stage_bytes = 0;

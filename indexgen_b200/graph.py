@@ -102,6 +102,17 @@ class Context:
               self.handle)
         return tuple(int(x.value) for x in v)
 
+    def set_coalescing(self, enable: bool):
+        """Build concurrent solve() calls on this context together (default)."""
+        check(lib().ig_ctx_set_coalescing(self.handle, int(bool(enable))), "ig_ctx_set_coalescing", self.handle)
+
+    def coalesce_stats(self):
+        """(batches, solve calls) that went through the combiner."""
+        b, r = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().ig_ctx_coalesce_stats(self.handle, ctypes.byref(b), ctypes.byref(r)), "ig_ctx_coalesce_stats",
+              self.handle)
+        return int(b.value), int(r.value)
+
     def set_autotune(self, enable: bool):
         check(lib().ig_ctx_set_autotune(self.handle, int(bool(enable))), "ig_ctx_set_autotune", self.handle)
 

@@ -1,0 +1,54 @@
+"""Concurrent solve() calls on one context (the reference's cluster worker
+pool calling its GPU path from several threads, src/SparseMat.cpp:978-1010)
+are built together and give every caller the codebook it gets alone.
+Integer work: bit-exact."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_concurrent_solves_equal_solo_solves():
+    from indexgen_b200 import Context, solve, workloads as W
+
+    jobs = [(W.uniform_words(n, L, 700 + i), L, d)
+            for i, (n, L, d) in enumerate([(4000, 12, 4), (2500, 10, 3), (6000, 14, 5), (900, 16, 9),
+                                           (3000, 11, 4), (0, 12, 4), (1, 12, 4), (5000, 13, 6),
+                                           (3500, 12, 4), (2000, 15, 5), (4500, 10, 4), (1200, 12, 2)])]
+    solo_ctx = Context(0)
+    try:
+        solo_ctx.set_coalescing(False)
+        want = [solve(w, L, d, 1, solo_ctx) for w, L, d in jobs]
+        assert solo_ctx.coalesce_stats() == (0, 0)
+    finally:
+        solo_ctx.close()
+    ctx = Context(0)
+    got = [None] * len(jobs)
+    errors = []
+    start = threading.Barrier(len(jobs))
+
+    def worker(i):
+        try:
+            w, L, d = jobs[i]
+            start.wait()
+            for _ in range(3):
+                got[i] = solve(w, L, d, 1, ctx)
+        except Exception as e:
+            errors.append((i, repr(e)))
+
+    try:
+        threads = [threading.Thread(target=worker, args=(i,)) for i in range(len(jobs))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert not errors, errors
+        for (book, edges), (wbook, wedges) in zip(got, want):
+            assert edges == wedges
+            assert np.array_equal(book, wbook)
+        batches, requests = ctx.coalesce_stats()
+        assert requests == 3 * len(jobs) and 1 <= batches <= requests
+    finally:
+        ctx.close()
