@@ -17,8 +17,10 @@ namespace ig {
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg)
 {
-    if (ctx)
+    if (ctx) {
+        std::lock_guard<std::mutex> lk(ctx->err_mu);
         ctx->last_error = msg;
+    }
     return s;
 }
 

@@ -97,6 +97,7 @@ struct Ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     std::mutex mu;
+    std::mutex err_mu;  // guards last_error (set_error runs with or without mu held)
     std::string last_error;
     int64_t launches = 0;
     // workspace

@@ -52,3 +52,41 @@ def test_concurrent_solves_equal_solo_solves():
         assert requests == 3 * len(jobs) and 1 <= batches <= requests
     finally:
         ctx.close()
+
+
+def test_bad_call_among_concurrent_solves():
+    """An invalid call fails on its own; the calls around it are built and
+    solved as usual."""
+    from indexgen_b200 import Context, IndexGenError, solve, workloads as W
+
+    ctx = Context(0)
+    good = [(W.uniform_words(2000 + 100 * i, 12, 60 + i), 12, 4) for i in range(4)]
+    want = []
+    try:
+        ctx.set_coalescing(False)
+        want = [solve(w, L, d, 1, ctx) for w, L, d in good]
+        ctx.set_coalescing(True)
+        results, errors = {}, {}
+        start = threading.Barrier(len(good) + 1)
+
+        def ok(i):
+            start.wait()
+            results[i] = solve(*good[i], 1, ctx)
+
+        def bad():
+            start.wait()
+            try:
+                solve(np.zeros(10, np.uint32), 17, 4, 1, ctx)  # length 17 is out of range
+            except IndexGenError as e:
+                errors["bad"] = e
+
+        threads = [threading.Thread(target=ok, args=(i,)) for i in range(len(good))] + [threading.Thread(target=bad)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        assert "bad" in errors and errors["bad"].code == "IG_ERR_INPUT"
+        for i, (book, edges) in enumerate(want):
+            assert results[i][1] == edges and np.array_equal(results[i][0], book)
+    finally:
+        ctx.close()

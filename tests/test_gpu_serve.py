@@ -58,3 +58,18 @@ def test_server_concurrent_submitters_and_cancel(igctx):
         else:
             got, _, _ = sv.wait(extra)
             assert np.array_equal(got, solo[3])
+
+
+def test_server_with_threaded_neighbour_order(igctx):
+    """A server whose greedies follow FillAdjList's order for 3 threads (the
+    host-assembled order, downloaded synchronously) gives ig_solve's results
+    for that order."""
+    from indexgen_b200 import Server, solve, workloads as W
+
+    jobs = [(W.uniform_words(n, L, 40 + n), L, d) for n, L, d in ((3000, 12, 4), (1500, 10, 3), (4000, 13, 5))]
+    solo = [solve(w, L, d, 3, igctx) for w, L, d in jobs]
+    with Server(igctx, host_threads=2, order_threads=3) as sv:
+        tickets = [sv.submit(w, L, d) for w, L, d in jobs]
+        for tk, (order, edges) in zip(tickets, solo):
+            got, e, _ = sv.wait(tk)
+            assert e == edges and np.array_equal(got, order)
