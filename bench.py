@@ -567,6 +567,7 @@ def run_ours(args, wl, rank, world, dist):
         e1.record(ext)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
+        seg_width, segments = G.job_tiling(0)
         G.close()
     torch.cuda.synchronize()
     launches = ctx.launches - launches0
@@ -620,7 +621,11 @@ def run_ours(args, wl, rank, world, dist):
     survey_achieved = survey_ops / pair_avg_s / 1e12 if pair_launches else None
     traffic = profile_traffic(wl["name"])
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
-    comp_bytes = 16 * edges + 4 * edges + 24 * (n + 1)
+    # compaction: 8 B edge record read + 4 B column written per edge, 4 B
+    # count read + 4 B prefix written per (row, segment) cell, 24 B per row
+    # (degree, offset scan, offset read)
+    cells = segments * n
+    comp_bytes = 12 * edges + 8 * cells + 24 * (n + 1)
     comp_avg_s = (comp_ms / max(comp_launches, 1)) / 1e3
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -645,7 +650,8 @@ def run_ours(args, wl, rank, world, dist):
         "compaction": {"bound": "hbm", "achieved": comp_bytes / comp_avg_s / 1e9 if comp_launches else None,
                        "peak": hbm_peak, "unit": "GB/s",
                        "frac": (comp_bytes / comp_avg_s / 1e9 / hbm_peak) if comp_launches else None,
-                       "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs"},
+                       "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs",
+                       "bytes_per_launch": comp_bytes, "count_cells": cells, "segment_width": seg_width},
         "gpu_launches": launches,
         "work_split": {"lane_form": ["full", "nibble", "byte"][lane_form(L, d)],
                        "items_per_cta": ctx.work_split(lane_form(L, d))[0],

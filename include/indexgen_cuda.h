@@ -106,6 +106,24 @@ ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_ct
 ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned);
 /* Automatic tuning on (1, default) or off (0). */
 ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable);
+/* Bound on every device-side wait of the pair kernels, in SM clock cycles
+ * (0 restores the default, about 2 s at 1.965 GHz).  A wait that runs out ends
+ * the build with IG_ERR_TIMEOUT after the CTA's copies in flight have landed;
+ * the context stays usable.  Replaces the reference's unbounded waits on its
+ * python3 subprocess (src/SparseMat.cpp:500-513). */
+ig_status ig_ctx_set_wait_limit(ig_ctx *ctx, int64_t cycles);
+/* Fault injection for tests of the failure paths; nothing here faults the
+ * GPU, each kind fires once:
+ *   IG_FAULT_NONE          clears any pending injection;
+ *   IG_FAULT_DEVICE_ALLOC  the arg-th device allocation this context makes
+ *                          from now on (arg >= 1) fails as out of memory;
+ *   IG_FAULT_TILE_COPY     the next pair pass does not issue the copy of the
+ *                          first staged tile of each pair kernel's first work
+ *                          item, so that tile's bounded wait runs out. */
+#define IG_FAULT_NONE 0
+#define IG_FAULT_DEVICE_ALLOC 1
+#define IG_FAULT_TILE_COPY 2
+ig_status ig_ctx_inject_fault(ig_ctx *ctx, int kind, int64_t arg);
 /* Concurrent ig_solve calls built together (1, default) or one by one (0),
  * and how many batches and calls have gone through the combiner. */
 ig_status ig_ctx_set_coalescing(ig_ctx *ctx, int enable);
@@ -185,6 +203,12 @@ ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
                          const int32_t *lens, const int32_t *min_eds, int words_on_device, ig_graph **out);
 ig_status ig_graph_job_count(const ig_graph *g, int32_t *jobs);
 ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word, int32_t *n, int64_t *edges);
+/* Tiling the pair pass used for job j: column segments of segment_width
+ * columns (a power of two, at most 65,536) and their number; each (row,
+ * segment) pair had one count cell.  Zero for jobs without pair tests and for
+ * graphs read from a file.  The replacement of the reference's fixed
+ * 16384 x 16384 tiles (src/cuda_edit_distance.py:380-390). */
+ig_status ig_graph_job_tiling(const ig_graph *g, int32_t job, int32_t *segment_width, int32_t *segments);
 /* Greedy of every job on host_threads host threads (0 = all cores), largest
  * job first.  Job j's codebook, as job-local vertex ids in selection order,
  * is written to order + offsets[j]; counts[j] is its size.  order_threads as

@@ -9,6 +9,9 @@ nearest-centre assignment of src/gpu_cluster.py).
 from .graph import (  # noqa: F401
     ConflictGraph,
     Context,
+    FAULT_DEVICE_ALLOC,
+    FAULT_NONE,
+    FAULT_TILE_COPY,
     IndexGenError,
     LANES_BYTE,
     LANES_FULL,

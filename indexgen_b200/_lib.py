@@ -21,11 +21,12 @@ EXPORTS = (
     "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
     "ig_assign_centers", "ig_cluster_solve", "ig_graph_write_adj_list", "ig_graph_read_adj_list",
-    "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_codebooks", "ig_solve_batch",
+    "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_tiling", "ig_graph_job_codebooks", "ig_solve_batch",
     "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
     "ig_server_stats", "ig_server_destroy",
     "ig_lane_form", "ig_ctx_autotune", "ig_ctx_set_work_split", "ig_ctx_work_split", "ig_ctx_set_autotune",
     "ig_ctx_set_graphs", "ig_ctx_graph_stats", "ig_ctx_set_coalescing", "ig_ctx_coalesce_stats",
+    "ig_ctx_set_wait_limit", "ig_ctx_inject_fault",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -91,6 +92,7 @@ def _declare(L):
         "ig_batch_build": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, ctypes.POINTER(_vp)]),
         "ig_graph_job_count": (_int, [_vp, ctypes.POINTER(_i32)]),
         "ig_graph_job_stats": (_int, [_vp, _i32, ctypes.POINTER(_i64), ctypes.POINTER(_i32), ctypes.POINTER(_i64)]),
+        "ig_graph_job_tiling": (_int, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32)]),
         "ig_graph_job_codebooks": (_int, [_vp, _int, _int, _vp, _vp]),
         "ig_solve_batch": (_int, [_vp, _vp, _vp, _i32, _vp, _vp, _int, _int, _vp, _vp, _vp]),
         "ig_server_create": (_int, [_vp, ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)]),
@@ -109,6 +111,8 @@ def _declare(L):
         "ig_ctx_set_graphs": (_int, [_vp, _int]),
         "ig_ctx_graph_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
         "ig_ctx_set_coalescing": (_int, [_vp, _int]),
+        "ig_ctx_set_wait_limit": (_int, [_vp, _i64]),
+        "ig_ctx_inject_fault": (_int, [_vp, _int, _i64]),
         "ig_ctx_coalesce_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
     }
     for name, (res, args) in sig.items():

@@ -198,19 +198,16 @@ __global__ void __launch_bounds__(kBigThreads) sort_lower_big(const int64_t *__r
             return cuda_error(ctx, e_, #call);                                                                 \
     } while (0)
 
-}  // namespace
-
-ig_status build_adjacency(Ctx *ctx, Graph *g)
+// The adjacency goes to fresh arrays that the graph takes only when every
+// step succeeded: a failed build (an allocation, a launch) frees them, so a
+// later request never sees a half-built adjacency.
+ig_status build_adjacency_into(Ctx *ctx, const Graph *g, int64_t *adj_ptr, int32_t *adj)
 {
-    if (g->d_adj_ptr)
-        return IG_OK;
     cudaStream_t st = ctx->stream;
     const int32_t n = g->n;
     const int64_t nnz = g->edges;
-    IG_CUDA(cudaMallocAsync((void **)&g->d_adj_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
-    IG_CUDA(cudaMallocAsync((void **)&g->d_adj, std::max<size_t>((size_t)(2 * nnz), 1) * sizeof(int32_t), st));
     if (n == 0 || nnz == 0) {
-        IG_CUDA(cudaMemsetAsync(g->d_adj_ptr, 0, ((size_t)n + 1) * sizeof(int64_t), st));
+        IG_CUDA(cudaMemsetAsync(adj_ptr, 0, ((size_t)n + 1) * sizeof(int64_t), st));
         IG_CUDA(cudaStreamSynchronize(st));
         return IG_OK;
     }
@@ -226,15 +223,15 @@ ig_status build_adjacency(Ctx *ctx, Graph *g)
     IG_CUDA(cudaMemsetAsync(nbig, 0, sizeof(int32_t), st));
     const int grid = ctx->sm_count * 8;
     lower_degree<<<grid, 256, 0, st>>>(g->d_cols, nnz, ldeg);
-    full_degree<<<(n + 256) / 256, 256, 0, st>>>(g->d_row_ptr, ldeg, n, g->d_adj_ptr);
+    full_degree<<<(n + 256) / 256, 256, 0, st>>>(g->d_row_ptr, ldeg, n, adj_ptr);
     ctx->launches += 2;
     IG_CUDA(cudaGetLastError());
-    s = inclusive_scan_i64(ctx, g->d_adj_ptr, (int64_t)n + 1);
+    s = inclusive_scan_i64(ctx, adj_ptr, (int64_t)n + 1);
     if (s != IG_OK)
         return s;
-    fill_rows<<<(unsigned)(((int64_t)n * 32 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, g->d_cols, n, g->d_adj_ptr,
-                                                                          ldeg, cursor, g->d_adj);
-    sort_lower_small<<<(n + 7) / 8, 256, 0, st>>>(g->d_adj_ptr, ldeg, n, g->d_adj, big, nbig);
+    fill_rows<<<(unsigned)(((int64_t)n * 32 + 255) / 256), 256, 0, st>>>(g->d_row_ptr, g->d_cols, n, adj_ptr, ldeg,
+                                                                          cursor, adj);
+    sort_lower_small<<<(n + 7) / 8, 256, 0, st>>>(adj_ptr, ldeg, n, adj, big, nbig);
     ctx->launches += 2;
     IG_CUDA(cudaGetLastError());
     int32_t host_nbig = 0;
@@ -245,15 +242,41 @@ ig_status build_adjacency(Ctx *ctx, Graph *g)
         s = ensure_buffer(ctx, ctx->records, (size_t)(2 * nnz) * sizeof(int32_t), "sort scratch");
         if (s != IG_OK)
             return s;
-        ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
         const size_t smem = kBitmapWords * sizeof(uint32_t);
         IG_CUDA(cudaFuncSetAttribute(sort_lower_big, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        sort_lower_big<<<host_nbig, kBigThreads, smem, st>>>(g->d_adj_ptr, ldeg, big, g->d_adj,
+        sort_lower_big<<<host_nbig, kBigThreads, smem, st>>>(adj_ptr, ldeg, big, adj,
                                                               static_cast<int32_t *>(ctx->records.ptr));
         ctx->launches++;
         IG_CUDA(cudaGetLastError());
     }
     IG_CUDA(cudaStreamSynchronize(st));
+    return IG_OK;
+}
+
+}  // namespace
+
+ig_status build_adjacency(Ctx *ctx, Graph *g)
+{
+    if (g->d_adj_ptr)
+        return IG_OK;
+    cudaStream_t st = ctx->stream;
+    int64_t *adj_ptr = nullptr;
+    int32_t *adj = nullptr;
+    cudaError_t e = dev_malloc(ctx, (void **)&adj_ptr, ((size_t)g->n + 1) * sizeof(int64_t), st);
+    if (e == cudaSuccess)
+        e = dev_malloc(ctx, (void **)&adj, std::max<size_t>((size_t)(2 * g->edges), 1) * sizeof(int32_t), st);
+    ig_status s = e == cudaSuccess ? build_adjacency_into(ctx, g, adj_ptr, adj) : cuda_error(ctx, e, "adjacency arrays");
+    if (s != IG_OK) {
+        if (adj_ptr)
+            cudaFreeAsync(adj_ptr, st);
+        if (adj)
+            cudaFreeAsync(adj, st);
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+        return s;
+    }
+    g->d_adj_ptr = adj_ptr;
+    g->d_adj = adj;
     return IG_OK;
 }
 

@@ -24,6 +24,18 @@ ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg)
     return s;
 }
 
+cudaError_t dev_malloc(Ctx *ctx, void **p, size_t bytes, cudaStream_t st)
+{
+    int64_t left = ctx->fail_alloc_in.load();
+    while (left > 0 && !ctx->fail_alloc_in.compare_exchange_weak(left, left - 1)) {
+    }
+    if (left == 1) {  // this is the allocation chosen to fail (injected, once)
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMallocAsync(p, bytes, st);
+}
+
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what)
 {
     cudaGetLastError();
@@ -53,7 +65,7 @@ ig_status stage_words(Ctx *ctx, const uint32_t *words, int32_t n, int on_device,
             cudaFreeAsync(ctx->words.ptr, ctx->stream);
         ctx->words.ptr = nullptr;
         ctx->words.bytes = 0;
-        cudaError_t e = cudaMallocAsync(&ctx->words.ptr, bytes, ctx->stream);
+        cudaError_t e = dev_malloc(ctx, &ctx->words.ptr, bytes, ctx->stream);
         if (e != cudaSuccess)
             return cuda_error(ctx, e, "word buffer allocation");
         ctx->words.bytes = bytes;
@@ -241,7 +253,7 @@ bool reserve_pool(Ctx *ctx, size_t bytes)
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     void *p = nullptr;
-    cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
+    cudaError_t e = dev_malloc(ctx, &p, bytes, ctx->stream);
     if (e == cudaSuccess)
         e = cudaFreeAsync(p, ctx->stream);
     if (e == cudaSuccess)
@@ -812,19 +824,19 @@ ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges)
         return IG_ERR_INPUT;
     std::lock_guard<std::mutex> lk(ctx->mu);
     ig::DeviceGuard dg(ctx->device);
-    if ((unsigned long long)edges <= ctx->rec_capacity)
+    if ((unsigned long long)edges <= ig::rec_capacity(ctx))
         return IG_OK;
     if (ctx->records.ptr)
         cudaFreeAsync(ctx->records.ptr, ctx->stream);
     ctx->records.ptr = nullptr;
     ctx->records.bytes = 0;
-    ctx->rec_capacity = 0;
     const size_t bytes = (size_t)edges * sizeof(ig::EdgeRecord);
-    cudaError_t e = cudaMallocAsync(&ctx->records.ptr, bytes, ctx->stream);
-    if (e != cudaSuccess)
+    cudaError_t e = ig::dev_malloc(ctx, &ctx->records.ptr, bytes, ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->records.ptr = nullptr;
         return ig::cuda_error(ctx, e, "edge record reservation");
+    }
     ctx->records.bytes = bytes;
-    ctx->rec_capacity = (unsigned long long)edges;
     return IG_OK;
     IG_ABI_CATCH
 }
@@ -1017,6 +1029,20 @@ ig_status ig_graph_job_stats(const ig_graph *g, int32_t job, int64_t *first_word
         *n = g->jobs[(size_t)job].n;
     if (edges)
         *edges = g->job_edge_off[(size_t)job + 1] - g->job_edge_off[(size_t)job];
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_graph_job_tiling(const ig_graph *g, int32_t job, int32_t *segment_width, int32_t *segments)
+{
+    IG_ABI_TRY
+    if (!g || job < 0 || job >= (int32_t)g->jobs.size())
+        return IG_ERR_INPUT;
+    const bool known = (size_t)job < g->job_nseg.size();
+    if (segment_width)
+        *segment_width = known && g->job_nseg[(size_t)job] > 0 ? 1 << g->job_seg_shift[(size_t)job] : 0;
+    if (segments)
+        *segments = known ? g->job_nseg[(size_t)job] : 0;
     return IG_OK;
     IG_ABI_CATCH
 }
@@ -1316,6 +1342,42 @@ ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *inst
     if (updates)
         *updates = ctx->graph_updates;
     return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_set_wait_limit(ig_ctx *ctx, int64_t cycles)
+{
+    IG_ABI_TRY
+    if (!ctx || cycles < 0)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->wait_cycles = cycles == 0 ? ig::kDefaultWaitCycles : (long long)cycles;
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_inject_fault(ig_ctx *ctx, int kind, int64_t arg)
+{
+    IG_ABI_TRY
+    if (!ctx)
+        return IG_ERR_INPUT;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    switch (kind) {
+    case IG_FAULT_NONE:
+        ctx->fail_alloc_in.store(0);
+        ctx->fault_tile_copy = false;
+        return IG_OK;
+    case IG_FAULT_DEVICE_ALLOC:
+        if (arg < 1)
+            return IG_ERR_INPUT;
+        ctx->fail_alloc_in.store(arg);
+        return IG_OK;
+    case IG_FAULT_TILE_COPY:
+        ctx->fault_tile_copy = true;
+        return IG_OK;
+    default:
+        return IG_ERR_INPUT;
+    }
     IG_ABI_CATCH
 }
 

@@ -70,7 +70,7 @@ struct DevArray {
     ig_status alloc(Ctx *c, size_t bytes)
     {
         ctx = c;
-        const cudaError_t e = cudaMallocAsync(&p, std::max<size_t>(bytes, 256), c->stream);
+        const cudaError_t e = dev_malloc(c, &p, std::max<size_t>(bytes, 256), c->stream);
         return e == cudaSuccess ? IG_OK : cuda_error(c, e, "cluster-solve workspace");
     }
 };

@@ -49,11 +49,10 @@ using myers::nib;
 using myers::row_pools;
 
 constexpr unsigned kFull = 0xffffffffu;
-// Bound on an mbarrier wait (SM clock cycles, ~2 s) before a CTA gives up and
-// reports IG_ERR_TIMEOUT instead of spinning forever.
-constexpr long long kMaxWaitCycles = 4000000000ll;
 
-enum : int { kStatusOk = 0, kStatusTimeout = 1 };
+// Pass status word: a bounded wait ran out (the CTA left after its copies in
+// flight had landed), or, worse, a copy in flight never landed either.
+enum : int { kStatusOk = 0, kStatusTimeout = 1, kStatusCopyLost = 2 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
@@ -233,15 +232,17 @@ struct PairArgs {
     uint32_t *counts;
     int *status;
     int emit;
+    long long wait_cycles;  // bound on every mbarrier wait (SM clock cycles)
+    int skip_first_copy;    // test hook: withhold the first tile copy of the kernel's first item
 };
 
 // Record slots.  Each warp takes slots from the global counter in chunks of
 // kSlotChunk (one atomic per chunk instead of one per hit group: a single
 // counter address is otherwise the limit on dense graphs) and keeps the rest
 // of its chunk in shared memory.  Slots a warp never fills are written as
-// sentinels (row = kNoRow) when the kernel ends; the scatter skips them.
+// sentinels (cell = kNoCell) when the kernel ends; the scatter skips them.
 constexpr unsigned kSlotChunk = 64;
-constexpr uint32_t kNoRow = 0xffffffffu;
+constexpr uint32_t kNoCell = 0xffffffffu;
 
 // Two scalar arrays, each element read and written on its own (a 16-byte
 // struct here, read whole, faulted with a misaligned shared access).
@@ -316,13 +317,69 @@ __device__ __forceinline__ void warp_count_prefix(uint32_t cnt, int lane, unsign
     }
 }
 
+constexpr int kSlotVec = kTileCols * 2;  // uint4 per staged tile (8 KiB, every unit layout)
+
+// Thread 0: copy the tile of units starting at column c0 (at most kTile
+// columns, up to c_hi) into ring slot `slot`.
+template <int kTile, int kCols, int kVec>
+__device__ __forceinline__ void ring_issue(uint4 (*tile)[kSlotVec], uint64_t *bar, int slot, const uint4 *units,
+                                           int32_t c0, int32_t c_hi)
+{
+    const int nu = (min(kTile, c_hi - c0) + kCols - 1) / kCols;
+    const uint32_t bytes = (uint32_t)nu * kVec * 16;
+    mbar_arrive_expect_tx(&bar[slot], bytes);
+    bulk_g2s(&tile[slot][0], units + (size_t)(c0 / kCols) * kVec, bytes, &bar[slot]);
+}
+
+// Ring state bits: bit s (s = 0, 1) is the phase parity slot s waits for
+// next; kSkipped marks an item whose first tile copy the test hook withheld
+// (cleared by that tile's wait).
+constexpr uint32_t kSkipped = 4u;
+
+// A CTA whose wait on a staged tile ran out leaves its item loop, but not
+// before thread 0 has waited (bounded) for the copies it issued that may still
+// be in flight into the CTA's shared memory -- slot b's, unless the test hook
+// withheld it, and the other slot's, when the next tile was issued -- so that
+// no bulk copy lands after the CTA is gone.  The wait happens once per kernel,
+// after the item loop (ring_drain), where it costs the pair loop no
+// registers; ring_note_abort leaves it what it needs: bit 0 = slot b, bit 1 =
+// slot b's copy was issued, bit 2 = the other slot's copy was issued.
+__shared__ uint32_t g_drain;
+
+__device__ __forceinline__ void ring_note_abort(const PairArgs &a, int b, bool b_issued, bool other_issued)
+{
+    atomicCAS(a.status, kStatusOk, kStatusTimeout);
+    g_drain = (uint32_t)b | (b_issued ? 2u : 0u) | (other_issued ? 4u : 0u);
+}
+
+// Thread 0, after the item loop of an aborted CTA.  `parity` has slot b's bit
+// already advanced past the phase that timed out.  Waiting on a phase that
+// has completed returns at once; a copy that never lands is reported as
+// kStatusCopyLost.
+__device__ __forceinline__ void ring_drain(const PairArgs &a, uint64_t *bar, uint32_t parity)
+{
+    const uint32_t d = g_drain;
+    const int b = (int)(d & 1u);
+    const uint32_t pend = parity ^ (1u << b);  // the phase each slot still waits for
+    for (int slot = 0; slot < 2; ++slot) {
+        if (!((d >> (slot == b ? 1 : 2)) & 1u))
+            continue;
+        const long long t0 = clock64();
+        while (!mbar_try_wait(&bar[slot], (pend >> slot) & 1u)) {
+            if (clock64() - t0 > a.wait_cycles) {
+                atomicExch(a.status, kStatusCopyLost);
+                break;
+            }
+        }
+    }
+}
+
 // Everything one thread needs about its row while it walks a segment.
 struct RowCtx {
     int32_t row;     // job-local row
     bool ok;         // row < n
     uint32_t p01, p23;
-    uint32_t grow;   // global row
-    uint32_t base;   // global id of the job's column 0
+    int32_t seg0;    // job-local first column of the segment
     uint32_t cell;   // index of this (row, segment) count
     int32_t n;
     int lim;
@@ -365,7 +422,7 @@ __device__ __forceinline__ void emit_mask(const PairArgs &a, uint32_t m, const R
         m &= m - 1u;
         const unsigned long long idx = j < sl.n0 ? sl.b0 + j : sl.b1 + (j - sl.n0);
         if (idx < a.rec_cap) {
-            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(r.grow, r.base + (uint32_t)(col0 + c), rank, r.cell);
+            *reinterpret_cast<uint2 *>(a.rec + idx) = make_uint2(r.cell, (uint32_t)(col0 + c - r.seg0) << 16 | rank);
         }
         ++rank;
         ++j;
@@ -458,14 +515,11 @@ __device__ __forceinline__ void tile_pass_band(const PairArgs &a, const uint4 *t
     }
 }
 
-constexpr int kSlotVec = kTileCols * 2;  // uint4 per staged tile (8 KiB, every unit layout)
-
 // Column-unit geometry of a lane form.
 template <int L, int MODE>
 struct Geo {
     static constexpr int kCols = MODE == kModeFull ? Unit<L>::kCols : BandUnit<MODE>::kCols;
     static constexpr int kVec = MODE == kModeFull ? Unit<L>::kVec : BandUnit<MODE>::kVec;
-    static constexpr int kBytes = kVec * 16;
     static constexpr int kTile = MODE == kModeFull ? kTileCols : BandUnit<MODE>::kTileCols;
     static_assert(kTile / kCols * kVec <= kTileCols * 2, "a tile must fit one staging slot");
 };
@@ -485,8 +539,7 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     r.ok = r.row < J.n;
     r.n = J.n;
     r.lim = J.lim;
-    r.base = (uint32_t)J.word_off;
-    r.grow = (uint32_t)(J.word_off + r.row);
+    r.seg0 = seg << J.seg_shift;
     r.cell = (uint32_t)(J.count_off + (long long)seg * J.n + r.row);
     const uint32_t rword = a.words[J.word_off + (r.ok ? r.row : 0)];
     uint32_t W[MODE == kModeFull ? 1 : L];
@@ -512,22 +565,21 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
     const int ntiles = (c_hi - c_lo + G::kTile - 1) / G::kTile;
     const uint4 *units = a.units + J.unit_off;
     uint32_t rank = 0;
+    // test hook: the first tile of the kernel's first item is never copied
+    if (a.skip_first_copy && J.item_off == 0 && band == 0 && seg == 0)
+        parity |= kSkipped;
 
     if (tid == 0) {
-        for (int t = 0; t < 2 && t < ntiles; ++t) {
-            const int32_t c0 = c_lo + t * G::kTile;
-            const int nu = (min(G::kTile, c_hi - c0) + G::kCols - 1) / G::kCols;
-            const uint32_t bytes = (uint32_t)nu * G::kBytes;
-            mbar_arrive_expect_tx(&bar[t], bytes);
-            bulk_g2s(&tile[t][0], units + (size_t)(c0 / G::kCols) * G::kVec, bytes, &bar[t]);
-        }
+        for (int t = 0; t < 2 && t < ntiles; ++t)
+            if (!(t == 0 && (parity & kSkipped)))
+                ring_issue<G::kTile, G::kCols, G::kVec>(tile, bar, t, units, c_lo + t * G::kTile, c_hi);
     }
     for (int t = 0; t < ntiles; ++t) {
         const int b = t & 1;
         bool timed_out = false;
         const long long t_start = clock64();
         while (!mbar_try_wait(&bar[b], (parity >> b) & 1u)) {
-            if (clock64() - t_start > kMaxWaitCycles) {
+            if (clock64() - t_start > a.wait_cycles) {
                 timed_out = true;
                 break;
             }
@@ -536,10 +588,12 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
         // uniform decision: every thread leaves together if any gave up
         if (__syncthreads_or(timed_out)) {
             if (tid == 0)
-                atomicExch(a.status, kStatusTimeout);
+                ring_note_abort(a, b, !(t == 0 && (parity & kSkipped)), t + 1 < ntiles);
+            parity &= ~kSkipped;
             aborted = true;
             return;
         }
+        parity &= ~kSkipped;
         const int32_t c0 = c_lo + t * G::kTile;
         const int nu = (min(G::kTile, c_hi - c0) + G::kCols - 1) / G::kCols;
         if constexpr (MODE == kModeFull) {
@@ -554,13 +608,8 @@ __device__ __forceinline__ void run_item(const PairArgs &a, const JobDesc &J, in
                 tile_pass_band<L, MODE, false>(a, tile[b], nu, c0, r, W, q, rank, lane);
         }
         __syncthreads();
-        if (tid == 0 && t + 2 < ntiles) {
-            const int32_t cn = c_lo + (t + 2) * G::kTile;
-            const int nun = (min(G::kTile, c_hi - cn) + G::kCols - 1) / G::kCols;
-            const uint32_t bytes = (uint32_t)nun * G::kBytes;
-            mbar_arrive_expect_tx(&bar[b], bytes);
-            bulk_g2s(&tile[b][0], units + (size_t)(cn / G::kCols) * G::kVec, bytes, &bar[b]);
-        }
+        if (tid == 0 && t + 2 < ntiles)
+            ring_issue<G::kTile, G::kCols, G::kVec>(tile, bar, b, units, c_lo + (t + 2) * G::kTile, c_hi);
     }
     if (r.ok)
         a.counts[r.cell] = rank;
@@ -618,7 +667,7 @@ __device__ __forceinline__ void fill_slot_tails(const PairArgs &a)
     for (unsigned k = tid & 31; k < left; k += 32) {
         const unsigned long long idx = base + k;
         if (idx < a.rec_cap)
-            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(kNoRow, 0u, 0u, 0u);
+            *reinterpret_cast<uint2 *>(a.rec + idx) = make_uint2(kNoCell, 0u);
     }
 }
 
@@ -656,6 +705,8 @@ __device__ __forceinline__ void item_loop(const PairArgs &a, uint64_t *bar, long
             break;
         __syncthreads();
     }
+    if (aborted && tid == 0)
+        ring_drain(a, bar, parity);
     if (a.emit && !aborted)
         fill_slot_tails(a);
 }
@@ -700,6 +751,8 @@ __global__ void __launch_bounds__(kBandRows, 6) pair_kernel(PairArgs a)
             break;
         __syncthreads();
     }
+    if (aborted && tid == 0)
+        ring_drain(a, bar, parity);
     if (a.emit && !aborted)
         fill_slot_tails(a);
 }
@@ -717,7 +770,7 @@ __device__ __forceinline__ void write_hits(const PairArgs &a, uint32_t m, const 
         m &= m - 1u;
         const unsigned long long idx = j < sl.n0 ? sl.b0 + j : sl.b1 + (j - sl.n0);
         if (idx < a.rec_cap)
-            *reinterpret_cast<uint4 *>(a.rec + idx) = make_uint4(r.grow, r.base + (uint32_t)(col0 + c), rank, r.cell);
+            *reinterpret_cast<uint2 *>(a.rec + idx) = make_uint2(r.cell, (uint32_t)(col0 + c - r.seg0) << 16 | rank);
         ++rank;
         ++j;
     }
@@ -800,9 +853,7 @@ __device__ __forceinline__ void run_item_nib(const PairArgs &a, const JobDesc &J
     rb.ok = rb.row < J.n;
     ra.n = rb.n = J.n;
     ra.lim = rb.lim = J.lim;
-    ra.base = rb.base = (uint32_t)J.word_off;
-    ra.grow = (uint32_t)(J.word_off + ra.row);
-    rb.grow = ra.grow + 1u;
+    ra.seg0 = rb.seg0 = seg << J.seg_shift;
     ra.cell = (uint32_t)(J.count_off + (long long)seg * J.n + ra.row);
     rb.cell = ra.cell + 1u;
     uint32_t W2[L];
@@ -828,33 +879,35 @@ __device__ __forceinline__ void run_item_nib(const PairArgs &a, const JobDesc &J
     const int ntiles = (c_hi - c_lo + kTile - 1) / kTile;
     const uint4 *units = a.units + J.unit_off;
     uint32_t rank_a = 0, rank_b = 0;
+    // test hook: the first tile of the kernel's first item is never copied
+    if (a.skip_first_copy && J.item_off == 0 && band == 0 && seg == 0)
+        parity |= kSkipped;
 
     if (tid == 0) {
-        for (int t = 0; t < 2 && t < ntiles; ++t) {
-            const int32_t c0 = c_lo + t * kTile;
-            const int nu = (min(kTile, c_hi - c0) + BU::kCols - 1) / BU::kCols;
-            const uint32_t bytes = (uint32_t)nu * BU::kBytes;
-            mbar_arrive_expect_tx(&bar[t], bytes);
-            bulk_g2s(&tile[t][0], units + (size_t)(c0 / BU::kCols) * BU::kVec, bytes, &bar[t]);
-        }
+        for (int t = 0; t < 2 && t < ntiles; ++t)
+            if (!(t == 0 && (parity & kSkipped)))
+                ring_issue<kTile, BU::kCols, BU::kVec>(tile, bar, t, units, c_lo + t * kTile, c_hi);
     }
     for (int t = 0; t < ntiles; ++t) {
         const int b = t & 1;
         bool timed_out = false;
         const long long t_start = clock64();
         while (!mbar_try_wait(&bar[b], (parity >> b) & 1u)) {
-            if (clock64() - t_start > kMaxWaitCycles) {
+            if (clock64() - t_start > a.wait_cycles) {
                 timed_out = true;
                 break;
             }
         }
         parity ^= 1u << b;
+        // uniform decision: every thread leaves together if any gave up
         if (__syncthreads_or(timed_out)) {
             if (tid == 0)
-                atomicExch(a.status, kStatusTimeout);
+                ring_note_abort(a, b, !(t == 0 && (parity & kSkipped)), t + 1 < ntiles);
+            parity &= ~kSkipped;
             aborted = true;
             return;
         }
+        parity &= ~kSkipped;
         const int32_t c0 = c_lo + t * kTile;
         const int nu = (min(kTile, c_hi - c0) + BU::kCols - 1) / BU::kCols;
         if (check)
@@ -862,13 +915,8 @@ __device__ __forceinline__ void run_item_nib(const PairArgs &a, const JobDesc &J
         else
             tile_pass_nib<L, false>(a, tile[b], nu, c0, ra, rb, W2, q, rank_a, rank_b, lane);
         __syncthreads();
-        if (tid == 0 && t + 2 < ntiles) {
-            const int32_t cn = c_lo + (t + 2) * kTile;
-            const int nun = (min(kTile, c_hi - cn) + BU::kCols - 1) / BU::kCols;
-            const uint32_t bytes = (uint32_t)nun * BU::kBytes;
-            mbar_arrive_expect_tx(&bar[b], bytes);
-            bulk_g2s(&tile[b][0], units + (size_t)(cn / BU::kCols) * BU::kVec, bytes, &bar[b]);
-        }
+        if (tid == 0 && t + 2 < ntiles)
+            ring_issue<kTile, BU::kCols, BU::kVec>(tile, bar, b, units, c_lo + (t + 2) * kTile, c_hi);
     }
     if (ra.ok)
         a.counts[ra.cell] = rank_a;
@@ -1029,24 +1077,73 @@ __global__ void scan_add(int64_t *__restrict__ x, int64_t m, const int64_t *__re
             x[base + k] += add;
 }
 
-// The slot count comes from the pair pass's counter on the device (the
-// scatter is queued in the same graph, before the host has seen it); a pass
-// whose slots overflowed the record buffer is rerun, so it scatters nothing.
+// Job owning count cell v: the last job with count_off <= v (a job without
+// cells shares the next job's count_off and so never wins).
+__device__ __forceinline__ int find_job_by_cell(const JobDesc *jobs, int njobs, uint32_t v)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jobs[mid].count_off <= (long long)v)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// cols[row_ptr[row] + prefix[cell] + rank] = column, for every record.  The
+// cell gives the job, the segment and the row; the record's high half is the
+// column's offset in its segment.  The slot count comes from the pair pass's
+// counter on the device (the scatter is queued in the same graph, before the
+// host has seen it); a pass whose slots overflowed the record buffer is
+// rerun, so it scatters nothing, and so does a pass whose pair kernel
+// reported a timeout (its counts and records are incomplete).  Records are
+// read once, with the streaming hint (evict first), so that the columns being
+// written stay in L2 while their sectors fill; each thread keeps kScatterIlp
+// records in flight.  A record whose cell or destination lies outside the
+// arrays is skipped (sentinels, and nothing else on a complete pass).
+constexpr int kScatterIlp = 4;
+
+__device__ __forceinline__ void scatter_one(uint2 r, const JobDesc *__restrict__ jobs, int njobs,
+                                            unsigned long long ncells, const int64_t *__restrict__ row_ptr,
+                                            const uint32_t *__restrict__ counts, int32_t *__restrict__ cols,
+                                            unsigned long long col_cap)
+{
+    if (r.x >= ncells)
+        return;
+    const JobDesc &J = jobs[find_job_by_cell(jobs, njobs, r.x)];
+    const uint32_t local = r.x - (uint32_t)J.count_off;
+    const uint32_t seg = local / (uint32_t)J.n;
+    const uint32_t row = local - seg * (uint32_t)J.n;
+    const int64_t pos = row_ptr[J.word_off + row] + (int64_t)counts[r.x] + (int64_t)(r.y & 0xffffu);
+    if ((unsigned long long)pos < col_cap)
+        cols[pos] = (int32_t)(J.word_off + ((int64_t)seg << J.seg_shift) + (int64_t)(r.y >> 16));
+}
+
 __global__ void scatter_records(const EdgeRecord *__restrict__ rec, const unsigned long long *__restrict__ d_slots,
-                                unsigned long long cap, const int64_t *__restrict__ row_ptr,
-                                const uint32_t *__restrict__ counts, int32_t *__restrict__ cols)
+                                const int *__restrict__ status, unsigned long long cap, const JobDesc *__restrict__ jobs,
+                                int njobs, unsigned long long ncells, const int64_t *__restrict__ row_ptr,
+                                const uint32_t *__restrict__ counts, int32_t *__restrict__ cols,
+                                unsigned long long col_cap)
 {
     const unsigned long long nrec = *d_slots;
-    if (nrec > cap)
+    if (nrec > cap || *status != kStatusOk)
         return;
-    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < nrec;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        const uint4 r = *reinterpret_cast<const uint4 *>(rec + i);
-        if (r.x == kNoRow)
-            continue;
-        const int64_t pos = row_ptr[r.x] + (int64_t)counts[r.w] + (int64_t)r.z;
-        cols[pos] = (int32_t)r.y;
+    const uint2 *r2 = reinterpret_cast<const uint2 *>(rec);
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    for (; i + (kScatterIlp - 1) * stride < nrec; i += kScatterIlp * stride) {
+        uint2 r[kScatterIlp];
+#pragma unroll
+        for (int k = 0; k < kScatterIlp; ++k)
+            r[k] = __ldcs(r2 + i + k * stride);
+#pragma unroll
+        for (int k = 0; k < kScatterIlp; ++k)
+            scatter_one(r[k], jobs, njobs, ncells, row_ptr, counts, cols, col_cap);
     }
+    for (; i < nrec; i += stride)
+        scatter_one(__ldcs(r2 + i), jobs, njobs, ncells, row_ptr, counts, cols, col_cap);
 }
 
 ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
@@ -1063,11 +1160,11 @@ ig_status ensure(Ctx *ctx, DevBuf &b, size_t bytes, const char *what)
         b.ptr = nullptr;
         b.bytes = 0;
     }
-    cudaError_t e = cudaMallocAsync(&b.ptr, want, ctx->stream);
+    cudaError_t e = dev_malloc(ctx, &b.ptr, want, ctx->stream);
     if (e != cudaSuccess && want > bytes) {  // the headroom does not fit: the exact size may
         cudaGetLastError();
         want = std::max<size_t>(bytes, 256);
-        e = cudaMallocAsync(&b.ptr, want, ctx->stream);
+        e = dev_malloc(ctx, &b.ptr, want, ctx->stream);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -1294,6 +1391,7 @@ bool plan_batch(const std::vector<JobSpec> &jobs, int grid_gen, int grid_nib, co
 struct CompactOut {
     int64_t *row_ptr = nullptr;  // n + 1
     int32_t *cols = nullptr;     // room for min(record capacity, pair tests) columns
+    unsigned long long col_cap = 0;
     int32_t n = 0;
 };
 
@@ -1359,14 +1457,16 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
     a.status = reinterpret_cast<int *>(flags + 2);
     a.hit_count = flags + 3;
     a.rec = static_cast<EdgeRecord *>(ctx->records.ptr);
-    a.rec_cap = out ? ctx->rec_capacity : 0;
+    a.rec_cap = out ? rec_capacity(ctx) : 0;
     a.counts = static_cast<uint32_t *>(ctx->counts.ptr);
     a.emit = out ? 1 : 0;
+    a.wait_cycles = ctx->wait_cycles;
+    a.skip_first_copy = ctx->fault_tile_copy ? 1 : 0;
     const int grid_nib = ctx->pair_grid_nib;
     const unsigned prep_grid = (unsigned)((B.units + 255) / 256);
     const int n = out ? out->n : 0;
     // scatter grid: enough threads for the slots the pass can hand out
-    const unsigned long long cap = ctx->rec_capacity;
+    const unsigned long long cap = rec_capacity(ctx);
     const int sgrid = (int)std::min<unsigned long long>((std::min<unsigned long long>(cap, (unsigned long long)B.pairs) + 255) / 256 + 1,
                                                         (unsigned long long)ctx->sm_count * 16);
     const std::vector<uint64_t> sig = {
@@ -1376,7 +1476,9 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
         (uint64_t)(uintptr_t)ctx->counts.ptr, (uint64_t)a.emit, (uint64_t)B.items_gen, (uint64_t)B.items_nib,
         B.desc_nib.size(),           B.desc_gen.size(), (uint64_t)grid, (uint64_t)grid_nib,
         out ? (uint64_t)(uintptr_t)out->row_ptr : 0, out ? (uint64_t)(uintptr_t)out->cols : 0, (uint64_t)n,
-        (uint64_t)sgrid,             (uint64_t)(uintptr_t)ctx->scan_tmp.ptr};
+        (uint64_t)sgrid,             (uint64_t)(uintptr_t)ctx->scan_tmp.ptr, (uint64_t)B.counts,
+        out ? (uint64_t)out->col_cap : 0, (uint64_t)a.wait_cycles, (uint64_t)a.skip_first_copy};
+    ctx->fault_tile_copy = false;  // the injected fault is one-shot
     int64_t launched = 0;
     s = run_graph(ctx, out ? 0 : 1, sig, out ? "build pass" : "count pass", [&]() -> cudaError_t {
         launched = 0;
@@ -1427,9 +1529,10 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
             // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
             if (inclusive_scan_i64(ctx, out->row_ptr, m) != IG_OK)
                 return cudaErrorLaunchFailure;
-            scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), flags + 1, cap,
+            scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), flags + 1,
+                                                    a.status, cap, d_jobs, njobs, (unsigned long long)B.counts,
                                                     out->row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
-                                                    out->cols);
+                                                    out->cols, out->col_cap);
             launched++;
             if ((e = cudaGetLastError()) != cudaSuccess)
                 return e;
@@ -1449,8 +1552,13 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
         return s;
     IG_CUDA(cudaStreamSynchronize(st));
     phase_collect(ctx);
-    if (static_cast<int>(host_flags[2] & 0xffffffffu) == kStatusTimeout)
-        return set_error(ctx, IG_ERR_TIMEOUT, "pair kernel: staged tile never arrived (bounded wait expired)");
+    const int status = static_cast<int>(host_flags[2] & 0xffffffffu);
+    if (status == kStatusTimeout)
+        return set_error(ctx, IG_ERR_TIMEOUT, "pair kernel: a staged tile did not arrive within the wait limit");
+    if (status == kStatusCopyLost)
+        return set_error(ctx, IG_ERR_TIMEOUT,
+                         "pair kernel: a staged tile did not arrive within the wait limit, and a copy still in flight "
+                         "did not land either");
     *slots = host_flags[1];
     *hits = host_flags[3];
     if (bounds)
@@ -1464,6 +1572,8 @@ ig_status check_jobs(Ctx *ctx, const std::vector<JobSpec> &jobs)
     for (const JobSpec &j : jobs) {
         if (j.n < 0 || j.len < 1 || j.len > IG_MAX_LEN || j.word_off < 0)
             return set_error(ctx, IG_ERR_INPUT, "job: n >= 0 and 1 <= len <= 16 required");
+        if (j.n > kMaxJobWords)
+            return set_error(ctx, IG_ERR_CAPACITY, "a job holds at most 16,777,215 words");
         rows = std::max<int64_t>(rows, j.word_off + j.n);
     }
     if (rows > (int64_t)INT32_MAX)
@@ -1529,11 +1639,14 @@ PairPlan make_plan(int32_t n, long long target_items)
     p.n = n;
     // Segment width: a power of two >= one band, small enough that the job
     // yields about target_items items, large enough that at most 256 segments
-    // exist and the per-(row, segment) counts stay under 1 GiB.
+    // exist and the per-(row, segment) counts stay under 1 GiB where a
+    // segment of at most 2^16 columns allows it (an edge record holds the
+    // column offset and the rank in 16 bits each; jobs of up to 2^24 - 1
+    // words fit 256 such segments).
     int shift = 8;  // 256 columns
-    while (((int64_t)n + (1ll << shift) - 1) >> shift > 256)
+    while (shift < kMaxSegShift && ((int64_t)n + (1ll << shift) - 1) >> shift > 256)
         shift++;
-    while ((((int64_t)n + (1ll << shift) - 1) >> shift) * (int64_t)n * 4 > (1ll << 30))
+    while (shift < kMaxSegShift && (((int64_t)n + (1ll << shift) - 1) >> shift) * (int64_t)n * 4 > (1ll << 30))
         shift++;
     // Prefer wider segments (fewer per-item overheads) while the target holds.
     for (;;) {
@@ -1720,18 +1833,23 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
     g->n = n;
     g->jobs = jobs;
     g->job_edge_off.assign(jobs.size() + 1, 0);
-    IG_CUDA(cudaMallocAsync((void **)&g->d_row_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
+    g->job_seg_shift.clear();
+    g->job_nseg.clear();
+    for (const JobDesc &d : B.desc) {
+        g->job_seg_shift.push_back(d.seg_shift);
+        g->job_nseg.push_back(d.nseg);
+    }
+    IG_CUDA(dev_malloc(ctx, (void **)&g->d_row_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
     if (B.items == 0) {
         IG_CUDA(cudaMemsetAsync(g->d_row_ptr, 0, ((size_t)n + 1) * sizeof(int64_t), st));
         IG_CUDA(cudaStreamSynchronize(st));
         g->edges = 0;
         return IG_OK;
     }
-    if (ctx->rec_capacity == 0) {
+    if (rec_capacity(ctx) == 0) {
         s = ensure(ctx, ctx->records, (size_t)(1u << 22) * sizeof(EdgeRecord), "edge records");
         if (s != IG_OK)
             return s;
-        ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
     }
     unsigned long long slots = 0, total = 0;
     for (int attempt = 0;; ++attempt) {
@@ -1739,18 +1857,19 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         // the pass may fill (at most one per pair test), so the compaction
         // runs in the same graph as the pair kernels, before the host has
         // seen the edge count; the graph then gets an exact copy
-        const size_t col_cap = (size_t)std::min<unsigned long long>(ctx->rec_capacity, (unsigned long long)B.pairs);
+        const size_t col_cap = (size_t)std::min<unsigned long long>(rec_capacity(ctx), (unsigned long long)B.pairs);
         if ((s = ensure(ctx, ctx->cols_ws, std::max<size_t>(col_cap, 1) * sizeof(int32_t), "column workspace")) !=
             IG_OK)
             return s;
         CompactOut out;
         out.row_ptr = g->d_row_ptr;
         out.cols = static_cast<int32_t *>(ctx->cols_ws.ptr);
+        out.col_cap = ctx->cols_ws.bytes / sizeof(int32_t);
         out.n = n;
         s = run_pass(ctx, d_words, B, grid, &out, &slots, &total, g->job_edge_off.data());
         if (s != IG_OK)
             return s;
-        if (slots <= ctx->rec_capacity)
+        if (slots <= rec_capacity(ctx))
             break;
         if (attempt > 0)
             return set_error(ctx, IG_ERR_STATE, "record slots exceeded a buffer sized for them twice");
@@ -1762,7 +1881,6 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         s = ensure(ctx, ctx->records, want * sizeof(EdgeRecord), "edge records");
         if (s != IG_OK)
             return s;
-        ctx->rec_capacity = ctx->records.bytes / sizeof(EdgeRecord);
     }
     g->edges = (int64_t)total;
     const int njobs = (int)B.desc.size();
@@ -1777,7 +1895,7 @@ ig_status build_batch(Ctx *ctx, const uint32_t *d_words, const std::vector<JobSp
         ctx->cols_ws.bytes = 0;
         return IG_OK;
     }
-    IG_CUDA(cudaMallocAsync((void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
+    IG_CUDA(dev_malloc(ctx, (void **)&g->d_cols, std::max<size_t>((size_t)total, 1) * sizeof(int32_t), st));
     if (total > 0) {
         IG_CUDA(cudaMemcpyAsync(g->d_cols, ctx->cols_ws.ptr, (size_t)total * sizeof(int32_t), cudaMemcpyDeviceToDevice,
                                 st));

@@ -1,6 +1,7 @@
 // Internal declarations shared by the libindexgen_cuda translation units.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -38,12 +39,20 @@ namespace ig {
 constexpr int kBandRows = 256;
 constexpr int kTileCols = 256;
 
-// One emitted edge: global row, global column, rank of the column among the
-// row's hits in its (row, segment) cell, and the index of that cell's count.
-// Ranks make the CSR scatter order-exact without a sort.
+// One emitted edge, 8 bytes: the index of its (row, segment) count cell, and
+// pos = (column offset within the segment) << 16 | rank of the column among
+// the row's hits in that cell.  The cell gives the job, row and segment
+// (cell = count_off + segment * n + row), so the row and the global column
+// are recovered in the scatter; ranks make it order-exact without a sort.
+// Segments are at most 2^16 columns wide, so offset and rank fit 16 bits each.
 struct EdgeRecord {
-    uint32_t row, col, rank, cell;
+    uint32_t cell, pos;
 };
+constexpr int kMaxSegShift = 16;
+constexpr long long kDefaultWaitCycles = 4000000000ll;
+// Largest job: its count cells (at most 256 segments x n) must be indexable
+// by 32 bits.
+constexpr int32_t kMaxJobWords = (1 << 24) - 1;
 
 // One job of a batch as the device sees it.  Rows and columns of a job are
 // local (0..n-1); word_off maps them to the concatenated word array.
@@ -102,7 +111,6 @@ struct Ctx {
     int64_t launches = 0;
     // workspace
     DevBuf words, sel, counts, records, scan_tmp, flags, adj_tmp, jobs, aux, cols_ws;
-    unsigned long long rec_capacity = 0;  // records that fit in `records`
     int pair_grid = 0;                    // persistent CTAs of the pair kernel
     int pair_grid_nib = 0;                // ... of the nibble-lane pair kernel
     // work split per lane form (full Myers, nibble, byte lanes): target items
@@ -134,12 +142,25 @@ struct Ctx {
     std::mutex greedy_mu;
     std::shared_ptr<class GreedyPool> greedy_pool;
     // concurrent ig_solve calls built together (ig_api.cu)
-    bool coalesce = true;
+    std::atomic<bool> coalesce{true};
     std::shared_ptr<struct SolveCombiner> combiner;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
     size_t stage_bytes = 0;
+    // bound on every mbarrier wait of the pair kernels (SM clock cycles,
+    // about 2 s at 1.965 GHz unless ig_ctx_set_wait_limit lowers it)
+    long long wait_cycles = kDefaultWaitCycles;
+    // fault injection for failure-path tests (ig_ctx_inject_fault): the
+    // number of device allocations left before one fails (0 = off), and a
+    // pair pass that withholds the copy of one staged tile (both one-shot)
+    std::atomic<int64_t> fail_alloc_in{0};
+    bool fault_tile_copy = false;
 };
+
+// Edge records that fit the context's record buffer.  Derived from the
+// buffer itself, so that a failed (re)allocation, which leaves the buffer
+// empty, can never leave a stale capacity behind.
+inline unsigned long long rec_capacity(const Ctx *ctx) { return ctx->records.bytes / sizeof(EdgeRecord); }
 
 // Records an event pair around a phase when profiling is on.
 void phase_begin(Ctx *ctx, int phase);
@@ -152,6 +173,7 @@ struct Graph {
     int64_t edges = 0;
     std::vector<JobSpec> jobs;          // one entry for a single-job graph
     std::vector<int64_t> job_edge_off;  // [jobs+1] row_ptr at job boundaries
+    std::vector<int32_t> job_seg_shift, job_nseg;  // pair-pass tiling per job (0 when not built here)
     int64_t *d_row_ptr = nullptr;       // [n+1]
     int32_t *d_cols = nullptr;          // [edges], global column ids
     // host copies, filled on first use
@@ -315,6 +337,9 @@ struct DeviceGuard {
 };
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
+// Every device allocation of the library goes through here (stream-ordered),
+// so that ig_ctx_inject_fault can make a chosen one fail as out of memory.
+cudaError_t dev_malloc(Ctx *ctx, void **p, size_t bytes, cudaStream_t st);
 ig_status cuda_error(Ctx *ctx, cudaError_t e, const char *what);
 
 }  // namespace ig

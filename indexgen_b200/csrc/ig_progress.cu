@@ -229,7 +229,7 @@ ig_status write_adj_list(Ctx *ctx, Graph *g, const char *path, int64_t *bytes_ou
         return IG_OK;
     DevMem off;
     off.st = st;
-    PG_CUDA(cudaMallocAsync(&off.p, ((size_t)n + 1) * sizeof(int64_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&off.p, ((size_t)n + 1) * sizeof(int64_t), st));
     int64_t *d_off = static_cast<int64_t *>(off.p);
     PG_CUDA(cudaMemsetAsync(d_off, 0, sizeof(int64_t), st));
     row_text_bytes<<<(unsigned)(((int64_t)n * 32 + 255) / 256), 256, 0, st>>>(g->d_adj_ptr, g->d_adj, n, d_off);
@@ -253,7 +253,7 @@ ig_status write_adj_list(Ctx *ctx, Graph *g, const char *path, int64_t *bytes_ou
     }
     DevMem text;
     text.st = st;
-    PG_CUDA(cudaMallocAsync(&text.p, (size_t)std::max<int64_t>(max_chunk, 1), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&text.p, (size_t)std::max<int64_t>(max_chunk, 1), st));
     std::shared_ptr<void> pin = ctx->pinned->acquire((size_t)std::max<int64_t>(max_chunk, 1));
     std::unique_ptr<char[]> heap;
     char *host = static_cast<char *>(pin.get());
@@ -311,9 +311,9 @@ ig_status read_adj_list(Ctx *ctx, const char *path, Graph *g)
     for (DevMem *m : {&d_text, &d_blocks, &d_nl, &d_a, &d_b, &d_bad})
         m->st = st;
     const int64_t nblk = std::max<int64_t>((size + kParseChunk - 1) / kParseChunk, 1);
-    PG_CUDA(cudaMallocAsync(&d_text.p, (size_t)std::max<int64_t>(size, 1), st));
-    PG_CUDA(cudaMallocAsync(&d_blocks.p, (size_t)(nblk + 1) * sizeof(int64_t), st));
-    PG_CUDA(cudaMallocAsync(&d_bad.p, sizeof(int), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_text.p, (size_t)std::max<int64_t>(size, 1), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_blocks.p, (size_t)(nblk + 1) * sizeof(int64_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_bad.p, sizeof(int), st));
     PG_CUDA(cudaMemsetAsync(d_bad.p, 0, sizeof(int), st));
     PG_CUDA(cudaMemsetAsync(d_blocks.p, 0, sizeof(int64_t), st));
     if (size > 0)
@@ -329,9 +329,9 @@ ig_status read_adj_list(Ctx *ctx, const char *path, Graph *g)
     int64_t lines = 0;
     PG_CUDA(cudaMemcpyAsync(&lines, blocks + nblk, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     PG_CUDA(cudaStreamSynchronize(st));
-    PG_CUDA(cudaMallocAsync(&d_nl.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int64_t), st));
-    PG_CUDA(cudaMallocAsync(&d_a.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
-    PG_CUDA(cudaMallocAsync(&d_b.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_nl.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int64_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_a.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&d_b.p, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
     list_newlines<<<(unsigned)nblk, kParseThreads, 0, st>>>(text, size, blocks, static_cast<int64_t *>(d_nl.p));
     ctx->launches++;
     PG_CUDA(cudaGetLastError());
@@ -390,10 +390,10 @@ ig_status read_adj_list(Ctx *ctx, const char *path, Graph *g)
     g->edges = up[(size_t)n];
     g->jobs.push_back(JobSpec{0, n, 1, 0});
     g->job_edge_off[1] = g->edges;
-    PG_CUDA(cudaMallocAsync((void **)&g->d_row_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
-    PG_CUDA(cudaMallocAsync((void **)&g->d_cols, (size_t)std::max<int64_t>(g->edges, 1) * sizeof(int32_t), st));
-    PG_CUDA(cudaMallocAsync((void **)&g->d_adj_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
-    PG_CUDA(cudaMallocAsync((void **)&g->d_adj, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&g->d_row_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&g->d_cols, (size_t)std::max<int64_t>(g->edges, 1) * sizeof(int32_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&g->d_adj_ptr, ((size_t)n + 1) * sizeof(int64_t), st));
+    PG_CUDA(dev_malloc(ctx, (void **)&g->d_adj, (size_t)std::max<int64_t>(lines, 1) * sizeof(int32_t), st));
     PG_CUDA(cudaMemcpyAsync(g->d_row_ptr, up.data(), up.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     PG_CUDA(cudaMemcpyAsync(g->d_adj_ptr, ap.data(), ap.size() * sizeof(int64_t), cudaMemcpyHostToDevice, st));
     if (g->edges > 0)

@@ -74,7 +74,7 @@ int64_t footprint_estimate(int32_t n, int len, int min_ed)
     const long double edges = std::min<long double>(pairs, pairs * density_estimate(len, min_ed) * 2 + 1024);
     const long double nseg = std::min<long double>(256, std::max<long double>(1, n / 256.0));
     // words + units + segment counts + CSR offsets + records + columns + adjacency
-    return (int64_t)(4.0L * n + 32.0L * n + 4.0L * n * nseg + 16.0L * n + 16 * edges + 4 * edges + 8 * edges);
+    return (int64_t)(4.0L * n + 32.0L * n + 4.0L * n * nseg + 16.0L * n + 8 * edges + 4 * edges + 8 * edges);
 }
 
 }  // namespace

@@ -113,6 +113,16 @@ class Context:
               self.handle)
         return int(b.value), int(r.value)
 
+    def set_wait_limit(self, cycles: int):
+        """Bound on the pair kernels' device waits (SM cycles; 0 = default)."""
+        check(lib().ig_ctx_set_wait_limit(self.handle, int(cycles)), "ig_ctx_set_wait_limit", self.handle)
+
+    def inject_fault(self, kind: int, arg: int = 0):
+        """Arm a one-shot failure for a test (FAULT_DEVICE_ALLOC: the arg-th
+        device allocation fails; FAULT_TILE_COPY: the next pair pass withholds
+        one staged tile copy so its bounded wait runs out; FAULT_NONE clears)."""
+        check(lib().ig_ctx_inject_fault(self.handle, int(kind), int(arg)), "ig_ctx_inject_fault", self.handle)
+
     def set_autotune(self, enable: bool):
         check(lib().ig_ctx_set_autotune(self.handle, int(bool(enable))), "ig_ctx_set_autotune", self.handle)
 
@@ -215,6 +225,14 @@ class ConflictGraph:
               "ig_graph_job_stats")
         return int(f.value), int(n.value), int(e.value)
 
+    def job_tiling(self, job: int = 0):
+        """(segment width, segments) of the pair pass that built one job."""
+        w = ctypes.c_int32()
+        k = ctypes.c_int32()
+        check(lib().ig_graph_job_tiling(self.handle, int(job), ctypes.byref(w), ctypes.byref(k)),
+              "ig_graph_job_tiling")
+        return int(w.value), int(k.value)
+
     def job_codebooks(self, order_threads: int = 1, host_threads: int = 0):
         """Per-job codebooks (job-local ids in selection order), as a list."""
         k = self.jobs
@@ -261,6 +279,9 @@ class ConflictGraph:
 
 
 LANES_FULL, LANES_NIBBLE, LANES_BYTE = 0, 1, 2
+
+
+FAULT_NONE, FAULT_DEVICE_ALLOC, FAULT_TILE_COPY = 0, 1, 2
 
 
 def lane_form(L: int, min_ed: int) -> int:
@@ -613,7 +634,7 @@ def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
 
 
 __all__ = [
-    "Context", "ConflictGraph", "IndexGenError", "Server", "build_conflict_graph", "build_batch", "solve_batch",
+    "Context", "ConflictGraph", "IndexGenError", "Server", "FAULT_NONE", "FAULT_DEVICE_ALLOC", "FAULT_TILE_COPY", "build_conflict_graph", "build_batch", "solve_batch",
     "count_conflicts",
     "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",

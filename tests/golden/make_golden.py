@@ -1,7 +1,7 @@
 """Regenerate the golden fixtures in this directory from the REFERENCE's own code.
 
-Runs in a container that holds the reference sources (default /root/reference,
-override with IG_REFERENCE).  It builds oracle/_ref/ref_driver from those
+Runs in a container that holds the reference sources; IG_REFERENCE must name
+that checkout.  It builds oracle/_ref/ref_driver from those
 sources (oracle/Makefile, target `ref`) and records what the reference's C++
 path outputs:
 
@@ -42,7 +42,7 @@ sys.path.insert(0, ROOT)
 
 from indexgen_b200 import workloads as W  # noqa: E402
 
-REF = os.environ.get("IG_REFERENCE", "/root/reference")
+REF = os.environ.get("IG_REFERENCE", "")
 DRIVER = os.path.join(ROOT, "oracle", "_ref", "ref_driver")
 
 
@@ -294,6 +294,8 @@ def main():
     ap.add_argument("--skip-large", action="store_true")
     ap.add_argument("--only", default="")
     a = ap.parse_args()
+    if not REF:
+        sys.exit("IG_REFERENCE must name the reference checkout")
     sh("make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REF}")
     with tempfile.TemporaryDirectory() as tmp:
         steps = {"uniform11": lambda: make_uniform11(tmp), "small": lambda: make_small(tmp),

@@ -4,7 +4,7 @@ Runs the reference's own solve_assignments_cuda (src/gpu_cluster.py) on
 seeded inputs under Numba's CUDA simulator (NUMBA_ENABLE_CUDASIM=1; no GPU
 needed) and stores the packed words, centres and the reference assignments.
 
-    python tests/golden/make_golden_assign.py /root/reference
+    python tests/golden/make_golden_assign.py <reference checkout>
 
 Cases cover L = 4..16, centre counts 1..40, duplicated centres (ties must go
 to the lowest index, as np.argmin does) and words equal to a centre.
@@ -50,4 +50,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden_assign.py <reference checkout>")
+    main(sys.argv[1])
