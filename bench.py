@@ -517,6 +517,162 @@ def run_serve_section(ctx, jobs: int, nmax: int, rate: float = 50.0) -> dict:
             "identical_to_plain": bool(same)}
 
 
+# ----------------------------------------------- config 5: serving stream ---
+SERVE5 = dict(jobs=2000, seed=5, rate=50.0, nmin=5000, nmax=500000)
+
+
+def serve5_stream(procs: int, jobs: int = 0):
+    """The config-5 stream as stated: 2,000 jobs, Poisson arrivals at 50/s, n
+    uniform in 10..16, editDist uniform in 3..5, candidates log-uniform in
+    [5,000, 500,000] after the maxRun 3 / GC [0.3,0.7] filters (seed 5).  The
+    words of the jobs are drawn in a spawned process pool (the same seeded
+    draws as workloads.serving_stream, job by job)."""
+    import multiprocessing as mp
+
+    specs = W.serving_stream_specs(SERVE5["jobs"], SERVE5["seed"], SERVE5["rate"], SERVE5["nmin"], SERVE5["nmax"])
+    specs = specs[:jobs] if jobs else specs
+    with mp.get_context("spawn").Pool(max(1, procs)) as pool:
+        words = pool.map(W.serving_job_words, specs, chunksize=4)
+    return [(t, w, L, d) for (t, _, L, d, _), w in zip(specs, words)]
+
+
+def run_serve5(args):
+    """One JSON line for config 5: the continuous-batching server against the
+    plain path -- one job per launch (coalescing off), solved by as many host
+    threads as the server's greedy pool has, each taking the next arrived job
+    in arrival order (the reference's cluster worker pool pattern,
+    src/SparseMat.cpp:978-1010).  Both arms see the same arrival times;
+    latency = arrival to codebook on the host; jobs/s = jobs / (last
+    completion - first arrival)."""
+    t_gen = time.perf_counter()
+    cores = host_cores()
+    stream = serve5_stream(cores, args.serve5_jobs)
+    t_gen = time.perf_counter() - t_gen
+    import torch
+
+    from indexgen_b200 import Context, Server, solve
+
+    torch.cuda.set_device(0)
+    props = torch.cuda.get_device_properties(0)
+    bus = None
+    if hasattr(props, "pci_bus_id") and hasattr(props, "pci_domain_id") and hasattr(props, "pci_device_id"):
+        bus = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}"
+    pairs = sum(len(w) * (len(w) - 1) // 2 for _, w, _, _ in stream)
+    words_bytes = sum(4 * len(w) for _, w, _, _ in stream)
+    ctx = Context(0)
+    # warm-up (untimed): a few small jobs through both paths
+    warm = sorted(stream, key=lambda j: len(j[1]))[:16]
+    with Server(ctx, host_threads=cores) as sv:
+        for t in [sv.submit(w, L, d) for _, w, L, d in warm]:
+            sv.wait(t)
+    for _, w, L, d in warm:
+        solve(w, L, d, 1, ctx)
+    launches0 = ctx.launches
+    clocks = ClockSampler(bus)
+    clocks.start()
+    # ---- served
+    lat = [0.0] * len(stream)
+    books = [None] * len(stream)
+    edges = [0] * len(stream)
+    with Server(ctx, host_threads=cores) as sv:
+        tickets = [None] * len(stream)
+        submitted = threading.Event()
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i, (arr, w, L, d) in enumerate(stream):
+                dt = arr - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                tickets[i] = sv.submit(w, L, d)
+            submitted.set()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for i in range(len(stream)):
+            books[i], edges[i], lat[i] = sv.wait(tickets[i])
+        t_served = time.perf_counter() - t0 - stream[0][0]
+        st = sv.stats()
+    served_launches = ctx.launches - launches0
+    clk_served = clocks.stop()
+    ctx.close()  # its workspaces go back to the device pool for the plain arm
+    # ---- plain: one job per launch, worker threads in arrival order
+    ctx_plain = Context(0)
+    ctx_plain.set_coalescing(False)
+    clocks = ClockSampler(bus)
+    clocks.start()
+    lat_plain = [0.0] * len(stream)
+    same = [True] * len(stream)
+    nxt = [0]
+    lock = threading.Lock()
+    errors = []
+    t0 = time.perf_counter()
+
+    def worker():
+        while True:
+            with lock:
+                i = nxt[0]
+                nxt[0] += 1
+            if i >= len(stream):
+                return
+            arr, w, L, d = stream[i]
+            dt = arr - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            try:
+                book, _ = solve(w, L, d, 1, ctx_plain)
+            except Exception as e:  # reported in the line, never silently dropped
+                errors.append((i, repr(e)))
+                same[i] = False
+                continue
+            lat_plain[i] = 1e3 * (time.perf_counter() - t0 - arr)
+            same[i] = bool(np.array_equal(book, books[i]))
+
+    ws = [threading.Thread(target=worker) for _ in range(max(1, cores - 1))]
+    for t in ws:
+        t.start()
+    for t in ws:
+        t.join()
+    t_plain = time.perf_counter() - t0 - stream[0][0]
+    clk_plain = clocks.stop()
+    plain_launches = ctx_plain.launches
+    ctx_plain.close()
+    n_jobs = len(stream)
+    total_edges = int(sum(edges))
+    book_bytes = sum(4 * len(b) for b in books)
+    served = n_jobs / t_served
+    line = {
+        "metric": "served codebook jobs/s", "value": served, "unit": "jobs/s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": 1e3 * t_served, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "serve5_poisson50_n10-16_d3-5_N5k-500k" + (
+                       "" if n_jobs == SERVE5["jobs"] else f"_first{n_jobs}_jobs"),
+                   "desc": f"{n_jobs} jobs, Poisson 50/s (seed 5), n uniform 10..16, editDist uniform 3..5, "
+                           "candidates log-uniform [5000, 500000] after maxRun 3 / GC [0.3,0.7]",
+                   "pair_tests": pairs, "edges": total_edges, "parallelism": "replicas x1",
+                   "l2": "inputs (860 MB of words) larger than L2",
+                   "step": "one pass over the whole stream (warm-up: 16 small jobs through both paths)"},
+        "e2e": {"value": served, "unit": "jobs/s", "h2d_bytes_per_step": words_bytes, "d2h_bytes_per_step": book_bytes,
+                "note": "serving is end to end by definition: host words in through ig_server_submit, codebooks "
+                        "out through ig_server_wait, wall clock from the first arrival to the last codebook"},
+        "serve": {"served_jobs_per_s": served, "served_p50_ms": float(np.percentile(lat, 50)),
+                  "served_p99_ms": float(np.percentile(lat, 99)), "served_max_ms": float(max(lat)),
+                  "served_s": t_served, "plain_jobs_per_s": n_jobs / t_plain,
+                  "plain_p50_ms": float(np.percentile(lat_plain, 50)),
+                  "plain_p99_ms": float(np.percentile(lat_plain, 99)), "plain_max_ms": float(max(lat_plain)),
+                  "plain_s": t_plain, "speedup_jobs_per_s": t_plain / t_served,
+                  "batches": st["batches"], "max_batch_jobs": st["max_batch_jobs"],
+                  "served_gpu_launches": served_launches, "plain_gpu_launches": plain_launches,
+                  "plain": f"one job per launch (coalescing off), {max(1, cores - 1)} worker threads in arrival order",
+                  "host_threads": cores, "identical_to_plain": bool(all(same)), "plain_errors": errors[:5],
+                  "stream_generation_s": t_gen},
+        "gpu_launches": served_launches,
+        "clocks": clk_served, "clocks_plain": clk_plain,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args, wl, rank, world, dist):
     import ctypes
 
@@ -679,11 +835,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16"])
+    ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16", "serve5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-clusters section")
     ap.add_argument("--serve-jobs", type=int, default=200, help="jobs in the serving section (0 = skip)")
     ap.add_argument("--serve-nmax", type=int, default=50000, help="largest job (candidates) in the serving stream")
+    ap.add_argument("--serve5-jobs", type=int, default=0,
+                    help="serve5: only the first K jobs of the stream (a trial run; 0 = all 2,000)")
     ap.add_argument("--subset", type=int, default=0,
                     help="use a seeded random subset of this many words (profiling runs)")
     args = ap.parse_args()
@@ -691,6 +849,14 @@ def main():
         args.warmup = 3
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
+    if args.workload == "serve5":
+        if args.impl == "reference" or world > 1:
+            if rank == 0:
+                print(json.dumps({"impl": args.impl, "unavailable": "the config-5 serving stream is a one-GPU "
+                                  "comparison of the library's server with its own one-job-per-launch path"}))
+            return
+        run_serve5(args)
+        return
     wl = workload(args.workload)
     if args.subset and args.subset < len(wl["words"]):
         rng = np.random.default_rng(4321)

@@ -106,6 +106,15 @@ ig_status ig_ctx_set_work_split(ig_ctx *ctx, int lane_form, int32_t items_per_ct
 ig_status ig_ctx_work_split(ig_ctx *ctx, int lane_form, int32_t *items_per_cta, int *tuned);
 /* Automatic tuning on (1, default) or off (0). */
 ig_status ig_ctx_set_autotune(ig_ctx *ctx, int enable);
+/* Host memory that graphs downloaded for the greedy may hold at once on this
+ * context (0 restores the default, half of physical memory): a download
+ * waits until the graphs whose greedies are still running leave room, so
+ * concurrent callers, batch groups and served batches of dense graphs stay
+ * within it together (one graph larger than the limit goes ahead alone once
+ * nothing else is held).  ig_ctx_host_budget reports the limit and the bytes
+ * held now. */
+ig_status ig_ctx_set_host_budget(ig_ctx *ctx, int64_t bytes);
+ig_status ig_ctx_host_budget(ig_ctx *ctx, int64_t *limit, int64_t *used);
 /* Bound on every device-side wait of the pair kernels, in SM clock cycles
  * (0 restores the default, about 2 s at 1.965 GHz).  A wait that runs out ends
  * the build with IG_ERR_TIMEOUT after the CTA's copies in flight have landed;
@@ -120,6 +129,10 @@ ig_status ig_ctx_set_wait_limit(ig_ctx *ctx, int64_t cycles);
  *   IG_FAULT_TILE_COPY     the next pair pass does not issue the copy of the
  *                          first staged tile of each pair kernel's first work
  *                          item, so that tile's bounded wait runs out. */
+/* Device allocations this context has asked for so far (workspaces grow
+ * rarely and are reused, so a steady stream of builds adds only the graphs'
+ * own arrays); with IG_FAULT_DEVICE_ALLOC it tells a test which one to fail. */
+ig_status ig_ctx_alloc_stats(ig_ctx *ctx, int64_t *device_allocs);
 #define IG_FAULT_NONE 0
 #define IG_FAULT_DEVICE_ALLOC 1
 #define IG_FAULT_TILE_COPY 2

@@ -10,6 +10,8 @@
 #include <string>
 #include <thread>
 
+#include <unistd.h>
+
 #include "ig_internal.h"
 
 
@@ -24,8 +26,49 @@ ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg)
     return s;
 }
 
+std::shared_ptr<void> HostBudget::acquire(int64_t bytes)
+{
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_.wait(lk, [&] { return used_ == 0 || used_ + bytes <= limit_; });
+    used_ += bytes;
+    auto self = shared_from_this();
+    return std::shared_ptr<void>(reinterpret_cast<void *>(1), [self, bytes](void *) {
+        std::lock_guard<std::mutex> g(self->mu_);
+        self->used_ -= bytes;
+        self->cv_.notify_all();
+    });
+}
+
+void HostBudget::set_limit(int64_t limit)
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    limit_ = limit;
+    cv_.notify_all();
+}
+
+int64_t HostBudget::limit()
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    return limit_;
+}
+
+int64_t HostBudget::used()
+{
+    std::lock_guard<std::mutex> lk(mu_);
+    return used_;
+}
+
+int64_t default_host_budget()
+{
+    const long pages = sysconf(_SC_PHYS_PAGES), page = sysconf(_SC_PAGE_SIZE);
+    if (pages <= 0 || page <= 0)
+        return (int64_t)16 << 30;
+    return (int64_t)pages * page / 2;
+}
+
 cudaError_t dev_malloc(Ctx *ctx, void **p, size_t bytes, cudaStream_t st)
 {
+    ctx->device_allocs++;
     int64_t left = ctx->fail_alloc_in.load();
     while (left > 0 && !ctx->fail_alloc_in.compare_exchange_weak(left, left - 1)) {
     }
@@ -127,25 +170,45 @@ ig_status fetch_host(ig_graph *g)
     return IG_OK;
 }
 
+// One host block of `bytes` for a graph download (pinned when the pool has
+// room, else plain memory), holding `token` -- its share of the host budget,
+// taken by the caller before the context lock -- until the block is released.
+std::shared_ptr<void> host_block(Ctx *ctx, size_t bytes, std::shared_ptr<void> token)
+{
+    std::shared_ptr<void> block = ctx->pinned->acquire(bytes);
+    if (!block) {
+        void *p = std::malloc(bytes);  // uninitialised: the copy fills it
+        if (!p)
+            return nullptr;
+        block = std::shared_ptr<void>(p, std::free);
+    }
+    void *raw = block.get();
+    return std::shared_ptr<void>(raw, [block, token](void *) mutable {
+        block.reset();
+        token.reset();
+    });
+}
+
+size_t adjacency_host_bytes(const Graph *g)
+{
+    return ((size_t)g->n + 1) * sizeof(int64_t) + (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
+}
+
 // Canonical symmetric adjacency on the device (built once), then into one
-// host block (pinned when the pool has room): offsets first, then neighbours.
+// host block: offsets first, then neighbours.
 ig_status fetch_adjacency(ig_graph *g, HostGraph &hg)
 {
     ig::Ctx *ctx = g->ctx;
+    std::shared_ptr<void> token = ctx->host_budget->acquire((int64_t)adjacency_host_bytes(g));
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     ig_status s = build_adjacency(ctx, g);
     if (s != IG_OK)
         return s;
     const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
-    const size_t adj_bytes = (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
-    std::shared_ptr<void> block = ctx->pinned->acquire(ptr_bytes + adj_bytes);
-    if (!block) {
-        void *p = std::malloc(ptr_bytes + adj_bytes);  // uninitialised: the copy fills it
-        if (!p)
-            return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
-        block = std::shared_ptr<void>(p, std::free);
-    }
+    std::shared_ptr<void> block = host_block(ctx, adjacency_host_bytes(g), std::move(token));
+    if (!block)
+        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
     int64_t *ap = static_cast<int64_t *>(block.get());
     int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
     cudaError_t e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, ctx->stream);
@@ -193,6 +256,7 @@ ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *
 ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, cudaHostFn_t then, void *arg)
 {
     ig::Ctx *ctx = g->ctx;
+    std::shared_ptr<void> token = ctx->host_budget->acquire((int64_t)adjacency_host_bytes(g));
     std::lock_guard<std::mutex> lk(ctx->mu);
     DeviceGuard dg(ctx->device);
     ig_status s = build_adjacency(ctx, g);  // ends with the context stream idle
@@ -204,14 +268,9 @@ ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, c
         return cuda_error(ctx, e, "download stream");
     }
     const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
-    const size_t adj_bytes = (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
-    std::shared_ptr<void> block = ctx->pinned->acquire(ptr_bytes + adj_bytes);
-    if (!block) {
-        void *p = std::malloc(ptr_bytes + adj_bytes);
-        if (!p)
-            return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
-        block = std::shared_ptr<void>(p, std::free);
-    }
+    std::shared_ptr<void> block = host_block(ctx, adjacency_host_bytes(g), std::move(token));
+    if (!block)
+        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
     int64_t *ap = static_cast<int64_t *>(block.get());
     int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
     cudaEvent_t fin = nullptr;
@@ -311,6 +370,8 @@ ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
     hg.job_edge_off = g->job_edge_off;
     if (order_threads == 1)
         return fetch_adjacency(g, hg);
+    std::shared_ptr<void> token = g->ctx->host_budget->acquire(
+        (int64_t)(((size_t)g->n + 1) * sizeof(int64_t) + (size_t)g->edges * sizeof(int32_t)));
     ig_status s = fetch_host(g);
     if (s != IG_OK)
         return s;
@@ -318,7 +379,10 @@ ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
         auto csr = std::make_shared<std::pair<std::vector<int64_t>, std::vector<int32_t>>>(g->h_row_ptr, g->h_cols);
         hg.ptr = csr->first.data();
         hg.idx = csr->second.data();
-        hg.storage = std::move(csr);
+        hg.storage = std::shared_ptr<void>(csr.get(), [csr, token](void *) mutable {
+            csr.reset();
+            token.reset();
+        });
     } catch (...) {
         return set_error(g->ctx, IG_ERR_OOM, "host CSR copy failed");
     }
@@ -491,6 +555,40 @@ std::shared_ptr<SolveCombiner> solve_combiner(Ctx *ctx)
     if (!ctx->combiner)
         ctx->combiner = std::make_shared<SolveCombiner>();
     return ctx->combiner;
+}
+
+// The waiting requests one coalesced build takes, in arrival order: the
+// first always, more while the batch stays within 2^36 pair tests (about
+// 0.1 s of device work) and 2^26 words; the rest wait for the next build.
+void take_coalesced(std::vector<SolveRequest *> &pending, std::vector<SolveRequest *> &batch)
+{
+    long double pairs = 0;
+    int64_t words = 0;
+    size_t k = 0;
+    for (; k < pending.size(); ++k) {
+        const SolveRequest *r = pending[k];
+        const long double p = (long double)r->n * (r->n > 0 ? r->n - 1 : 0) / 2;
+        if (k > 0 && (pairs + p > (long double)(1ull << 36) || words + r->n > ((int64_t)1 << 26)))
+            break;
+        pairs += p;
+        words += r->n;
+    }
+    batch.assign(pending.begin(), pending.begin() + (long)k);
+    pending.erase(pending.begin(), pending.begin() + (long)k);
+}
+
+void build_requests(ig_ctx *ctx, const std::vector<SolveRequest *> &reqs);
+
+// A merged build can fail where each request alone would not (its summed
+// workspace or a per-launch limit): those requests are then built one by
+// one, and each keeps its own outcome.
+void build_requests_or_split(ig_ctx *ctx, const std::vector<SolveRequest *> &reqs)
+{
+    build_requests(ctx, reqs);
+    if (reqs.size() < 2 || (reqs[0]->status != IG_ERR_OOM && reqs[0]->status != IG_ERR_CAPACITY))
+        return;
+    for (SolveRequest *r : reqs)
+        build_requests(ctx, {r});
 }
 
 // Builds the requests as one batch and downloads its canonical adjacency.
@@ -676,6 +774,47 @@ ig_status job_codebooks_impl(ig_graph *g, int order_threads, int host_threads, i
 }
 
 }  // namespace
+}  // namespace ig
+
+namespace ig {
+
+ig_status estimate_edges(Ctx *ctx, const std::vector<SampleJob> &jobs, std::vector<long double> &edges)
+{
+    edges.assign(jobs.size(), 0.0L);
+    std::vector<uint32_t> words;
+    std::vector<JobSpec> spec;
+    std::vector<long double> scale;
+    for (const SampleJob &j : jobs) {
+        const int32_t S = std::min<int32_t>(j.n, kSampleWords);
+        spec.push_back(JobSpec{(int64_t)words.size(), S, j.len, j.min_ed});
+        for (int32_t i = 0; i < S; ++i)
+            words.push_back(j.words[(int64_t)i * j.n / S]);
+        scale.push_back(S == j.n || S < 2 ? 1.0L
+                                          : (long double)j.n * (j.n - 1) / ((long double)S * (S - 1)));
+    }
+    if (words.empty())
+        return IG_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if (!dg.ok)
+        return set_error(ctx, IG_ERR_CUDA, "cannot select the context's device");
+    ig_graph *g = new (std::nothrow) ig_graph();
+    if (!g)
+        return IG_ERR_OOM;
+    const uint32_t *d_words = nullptr;
+    ig_status s = stage_words(ctx, words.data(), (int32_t)words.size(), 0, &d_words);
+    const bool tune = ctx->autotune;
+    ctx->autotune = false;  // samples must not pick the work split of real batches
+    if (s == IG_OK)
+        s = build_batch(ctx, d_words, spec, g);
+    ctx->autotune = tune;
+    if (s == IG_OK)
+        for (size_t k = 0; k < jobs.size(); ++k)
+            edges[k] = (long double)(g->job_edge_off[k + 1] - g->job_edge_off[k]) * scale[k];
+    release_graph(g, true);
+    return s;
+}
+
 }  // namespace ig
 
 extern "C" {
@@ -1090,6 +1229,7 @@ ig_status ig_batch_build(ig_ctx *ctx, const uint32_t *words, const int64_t *offs
     IG_ABI_CATCH
 }
 
+
 ig_status ig_solve_batch(ig_ctx *ctx, const uint32_t *words, const int64_t *offsets, int32_t jobs,
                          const int32_t *lens, const int32_t *min_eds, int order_threads, int host_threads,
                          int32_t *order, int32_t *counts, int64_t *edges)
@@ -1209,12 +1349,12 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
             std::unique_lock<std::mutex> lk(C->mu);
             C->pending.push_back(&req);
             while (!req.ready) {
-                if (!C->building) {  // the device is free: build everything that waits
+                if (!C->building) {  // the device is free: build what waits, up to a cap
                     C->building = true;
                     std::vector<ig::SolveRequest *> batch;
-                    batch.swap(C->pending);
+                    ig::take_coalesced(C->pending, batch);
                     lk.unlock();
-                    ig::build_requests(ctx, batch);
+                    ig::build_requests_or_split(ctx, batch);
                     lk.lock();
                     for (ig::SolveRequest *r : batch)
                         r->ready = true;
@@ -1240,9 +1380,15 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
         return s;
     if (edges)
         *edges = g->edges;
-    s = ig_graph_codebook(g, order_threads, order, count);
+    // the device graph goes before the greedy runs: concurrent callers then
+    // hold host copies only, within the context's host budget
+    ig::HostGraph hg;
+    s = ig::download_for_greedy(g, order_threads, hg);
     ig::release_graph(g);
-    return s;
+    if (s != IG_OK)
+        return s;
+    *count = ig::greedy_one(hg, 0, order);
+    return IG_OK;
     IG_ABI_CATCH
 }
 
@@ -1341,6 +1487,39 @@ ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *inst
         *instantiations = ctx->graph_instantiations;
     if (updates)
         *updates = ctx->graph_updates;
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_alloc_stats(ig_ctx *ctx, int64_t *device_allocs)
+{
+    IG_ABI_TRY
+    if (!ctx || !device_allocs)
+        return IG_ERR_INPUT;
+    *device_allocs = ctx->device_allocs.load();
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_set_host_budget(ig_ctx *ctx, int64_t bytes)
+{
+    IG_ABI_TRY
+    if (!ctx || bytes < 0)
+        return IG_ERR_INPUT;
+    ctx->host_budget->set_limit(bytes == 0 ? ig::default_host_budget() : bytes);
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_host_budget(ig_ctx *ctx, int64_t *limit, int64_t *used)
+{
+    IG_ABI_TRY
+    if (!ctx)
+        return IG_ERR_INPUT;
+    if (limit)
+        *limit = ctx->host_budget->limit();
+    if (used)
+        *used = ctx->host_budget->used();
     return IG_OK;
     IG_ABI_CATCH
 }

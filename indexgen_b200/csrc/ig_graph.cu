@@ -1601,6 +1601,24 @@ ig_status inclusive_scan_i64(Ctx *ctx, int64_t *x, int64_t m)
 
 ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what) { return ensure(ctx, b, bytes, what); }
 
+size_t workspace_bytes(const Ctx *ctx)
+{
+    return ctx->sel.bytes + ctx->counts.bytes + ctx->records.bytes + ctx->cols_ws.bytes + ctx->adj_tmp.bytes;
+}
+
+void trim_workspaces(Ctx *ctx, size_t keep_bytes)
+{
+    if (workspace_bytes(ctx) <= keep_bytes)
+        return;
+    for (DevBuf *b : {&ctx->sel, &ctx->counts, &ctx->records, &ctx->cols_ws, &ctx->adj_tmp}) {
+        if (b->ptr)
+            cudaFreeAsync(b->ptr, ctx->stream);
+        b->ptr = nullptr;
+        b->bytes = 0;
+    }
+    cudaGetLastError();
+}
+
 void phase_begin(Ctx *ctx, int phase)
 {
     if (!ctx->profiling)

@@ -101,6 +101,29 @@ private:
     size_t total_ = 0;
 };
 
+// Host memory held by graphs downloaded for the greedy (canonical adjacency
+// or upper CSR), from the download until the last greedy that reads them has
+// finished.  A download waits until it fits the limit, so that concurrent
+// callers, batch groups and served batches of dense graphs cannot take more
+// host memory than the limit together; one request larger than the limit
+// waits until nothing else is held and then goes ahead alone (ig_api.cu).
+class HostBudget : public std::enable_shared_from_this<HostBudget> {
+  public:
+    explicit HostBudget(int64_t limit) : limit_(limit) {}
+    // Blocks until `bytes` fit; the token releases them when its last copy goes.
+    std::shared_ptr<void> acquire(int64_t bytes);
+    void set_limit(int64_t limit);
+    int64_t limit();
+    int64_t used();
+
+  private:
+    std::mutex mu_;
+    std::condition_variable cv_;
+    int64_t limit_ = 0, used_ = 0;
+};
+// Default limit: half of the machine's physical memory.
+int64_t default_host_budget();
+
 struct Ctx {
     int device = 0;
     int sm_count = 0;
@@ -154,7 +177,9 @@ struct Ctx {
     // number of device allocations left before one fails (0 = off), and a
     // pair pass that withholds the copy of one staged tile (both one-shot)
     std::atomic<int64_t> fail_alloc_in{0};
+    std::atomic<int64_t> device_allocs{0};  // dev_malloc calls on this context
     bool fault_tile_copy = false;
+    std::shared_ptr<HostBudget> host_budget = std::make_shared<HostBudget>(default_host_budget());
 };
 
 // Edge records that fit the context's record buffer.  Derived from the
@@ -337,6 +362,25 @@ struct DeviceGuard {
 };
 
 ig_status set_error(Ctx *ctx, ig_status s, const std::string &msg);
+
+// Edge counts of jobs estimated from one batch build over a strided sample of
+// at most kSampleWords words of each job: exact for jobs no larger than the
+// sample, otherwise the sample's edges scaled by the pair ratio (the sample
+// pairs are a uniform draw from the job's pairs).  Used where memory must be
+// sized before a build, such as the server's admission (ig_api.cu).
+constexpr int32_t kSampleWords = 4096;
+struct SampleJob {
+    const uint32_t *words = nullptr;  // host
+    int32_t n = 0;
+    int32_t len = 1, min_ed = 0;
+};
+ig_status estimate_edges(Ctx *ctx, const std::vector<SampleJob> &jobs, std::vector<long double> &edges);
+// Frees the context's pair-pass workspaces (column streams, count cells, edge
+// records, column workspace, adjacency scratch) when together they hold more
+// than keep_bytes; the freed memory stays in the device pool for the next
+// allocations, and the workspaces grow again on demand (ig_graph.cu).
+void trim_workspaces(Ctx *ctx, size_t keep_bytes);
+size_t workspace_bytes(const Ctx *ctx);
 // Every device allocation of the library goes through here (stream-ordered),
 // so that ig_ctx_inject_fault can make a chosen one fail as out of memory.
 cudaError_t dev_malloc(Ctx *ctx, void **p, size_t bytes, cudaStream_t st);

@@ -38,6 +38,9 @@ struct ServerJob {
     int64_t ticket = 0;
     std::vector<uint32_t> words;
     int32_t n = 0, len = 1, min_ed = 0;
+    bool estimated = false;   // est_edges and footprint are known
+    bool solo = false;        // build alone (a merged build that held it failed)
+    long double est_edges = 0;
     int64_t footprint = 0;
     long double pairs = 0;
     JobState state = kQueued;
@@ -54,27 +57,25 @@ struct GreedyTask {
     std::shared_ptr<ServerJob> job;
 };
 
-// Edge density P(ED < d) of filtered uniform strings, per (n, d), used only to
-// estimate how much HBM a job will need before its pairs are counted.
-double density_estimate(int len, int min_ed)
+// Device memory a job needs at its peak, from its (estimated) edge count:
+// words, column units and count cells (at most 256 segments per row), CSR
+// offsets and canonical adjacency offsets; then per edge 8 B of edge record
+// and 4 B of column while it builds, and the columns plus 8 B of canonical
+// adjacency (4 B each way) while its adjacency is built -- the record buffer
+// doubles as the sort scratch of long adjacency rows.  The estimate gets a
+// fifth more room, and the record-chunk tails of the launch a fixed allowance.
+int64_t device_footprint(int32_t n, long double edges)
 {
-    static const double tab[7][3] = {{6.3e-4, 6.8e-3, 4.6e-2}, {2.1e-4, 2.7e-3, 2.0e-2}, {5.0e-5, 8.3e-4, 7.5e-3},
-                                     {1.5e-5, 2.5e-4, 2.7e-3}, {5e-6, 1.0e-4, 1.0e-3},   {5e-6, 2.0e-5, 3.7e-4},
-                                     {5e-6, 5e-6, 1.2e-4}};
-    if (min_ed <= 0)
-        return 0.0;
-    if (len >= 10 && len <= 16 && min_ed >= 3 && min_ed <= 5)
-        return tab[len - 10][min_ed - 3];
-    return min_ed > len ? 1.0 : 0.05;  // outside the table: be generous
+    const long double nseg = std::min<long double>(256, std::max<long double>(1, n / 256.0L));
+    const long double e = edges * 1.2L + 65536;
+    return (int64_t)(4.0L * n + 32.0L * n + 4.0L * n * nseg + 24.0L * ((long double)n + 1) + 20.0L * e);
 }
 
-int64_t footprint_estimate(int32_t n, int len, int min_ed)
+// Device memory a built graph holds until it is freed: CSR offsets and
+// columns, adjacency offsets and lists.
+int64_t graph_bytes(const ig_graph *g)
 {
-    const long double pairs = (long double)n * (n > 0 ? n - 1 : 0) / 2;
-    const long double edges = std::min<long double>(pairs, pairs * density_estimate(len, min_ed) * 2 + 1024);
-    const long double nseg = std::min<long double>(256, std::max<long double>(1, n / 256.0));
-    // words + units + segment counts + CSR offsets + records + columns + adjacency
-    return (int64_t)(4.0L * n + 32.0L * n + 4.0L * n * nseg + 16.0L * n + 8 * edges + 4 * edges + 8 * edges);
+    return 16 * ((int64_t)g->n + 1) + 12 * g->edges;
 }
 
 }  // namespace
@@ -97,6 +98,7 @@ struct ig_server {
 
     void schedule_loop();
     void greedy_loop();
+    void trim();
 };
 
 // Host callback behind a batch's adjacency copy: the batch's jobs go to the
@@ -134,8 +136,16 @@ void ig_server::schedule_loop()
         pend_g = nullptr;
         pend_done = nullptr;
     };
+    auto fail_job = [&](const std::shared_ptr<ServerJob> &j, ig_status s) {  // mu held
+        j->state = kFailed;
+        j->status = s;
+        j->t_done = Clock::now();
+        ++failed;
+    };
     for (;;) {
         std::vector<std::shared_ptr<ServerJob>> batch;
+        std::vector<std::shared_ptr<ServerJob>> fresh;  // not estimated yet
+        bool settle = false;
         {
             std::unique_lock<std::mutex> lk(mu);
             if (queue.empty() && pend_g) {  // nothing to overlap with: settle the last batch
@@ -149,16 +159,55 @@ void ig_server::schedule_loop()
                 finish_pending();
                 return;
             }
+            for (auto &j : queue)
+                if (!j->estimated && j->state == kQueued && fresh.size() < 512)
+                    fresh.push_back(j);
+        }
+        // Admission needs each job's HBM footprint, which depends on its edge
+        // count: one count pass over strided samples of the new jobs gives it
+        // (exact for jobs of at most 4,096 words).
+        if (!fresh.empty()) {
+            std::vector<ig::SampleJob> smp;
+            for (auto &j : fresh)
+                smp.push_back(ig::SampleJob{j->words.data(), j->n, j->len, j->min_ed});
+            std::vector<long double> est;
+            const ig_status s = ig::estimate_edges(ctx, smp, est);
+            std::lock_guard<std::mutex> lk(mu);
+            for (size_t k = 0; k < fresh.size(); ++k) {
+                auto &j = fresh[k];
+                if (s != IG_OK) {
+                    if (j->state == kQueued)
+                        fail_job(j, s);
+                    continue;
+                }
+                j->est_edges = est[k];
+                j->footprint = device_footprint(j->n, est[k]);
+                j->estimated = true;
+                if (j->state == kQueued && j->footprint > opts.hbm_budget_bytes)
+                    fail_job(j, IG_ERR_OOM);  // this job alone does not fit the HBM budget
+            }
+            cv_done.notify_all();
+        }
+        {
+            std::unique_lock<std::mutex> lk(mu);
+            const int64_t pend_mem = pend_g ? graph_bytes(pend_g) : 0;
             int64_t mem = 0;
             long double pairs = 0;
             while (!queue.empty()) {
                 std::shared_ptr<ServerJob> j = queue.front();
-                if (j->state == kCancelled) {
+                if (j->state != kQueued) {  // cancelled or failed while queued
                     queue.pop_front();
                     continue;
                 }
+                if (!j->estimated)
+                    break;  // arrived during the estimate: next round
                 const bool first = batch.empty();
-                if (!first && ((int)batch.size() >= opts.max_batch_jobs || mem + j->footprint > opts.hbm_budget_bytes ||
+                const bool fits = mem + j->footprint + pend_mem <= opts.hbm_budget_bytes;
+                if (first && !fits && pend_mem > 0) {
+                    settle = true;  // room comes back once the previous batch is freed
+                    break;
+                }
+                if (!first && ((int)batch.size() >= opts.max_batch_jobs || !fits || j->solo ||
                                pairs + j->pairs > (long double)opts.max_batch_pairs))
                     break;
                 queue.pop_front();
@@ -166,7 +215,13 @@ void ig_server::schedule_loop()
                 mem += j->footprint;
                 pairs += j->pairs;
                 batch.push_back(j);
+                if (j->solo)
+                    break;
             }
+        }
+        if (settle) {
+            finish_pending();
+            continue;
         }
         if (batch.empty())
             continue;
@@ -174,16 +229,42 @@ void ig_server::schedule_loop()
         std::vector<uint32_t> words;
         std::vector<int64_t> off{0};
         std::vector<int32_t> lens, eds;
+        long double want_records = 0;
         for (auto &j : batch) {
             words.insert(words.end(), j->words.begin(), j->words.end());
             off.push_back(off.back() + j->n);
             lens.push_back(j->len);
             eds.push_back(j->min_ed);
+            want_records += j->est_edges;
+        }
+        // room for the estimated records up front (a short estimate costs a
+        // rerun of the pass, never a wrong result)
+        ig_status s = IG_OK;
+        {
+            const long double need = want_records * 1.2L + (1 << 20);
+            int64_t cap = 0;
+            {
+                std::lock_guard<std::mutex> lk(ctx->mu);
+                cap = (int64_t)ig::rec_capacity(ctx);
+            }
+            if ((long double)cap < need)
+                s = ig_ctx_reserve(ctx, (int64_t)need);
         }
         ig_graph *g = nullptr;
-        ig_status s = ig_batch_build(ctx, words.data(), off.data(), (int32_t)batch.size(), lens.data(), eds.data(), 0,
-                                     &g);
+        if (s == IG_OK)
+            s = ig_batch_build(ctx, words.data(), off.data(), (int32_t)batch.size(), lens.data(), eds.data(), 0, &g);
         finish_pending();  // the previous batch's copy ran during this build
+        if ((s == IG_ERR_OOM || s == IG_ERR_CAPACITY) && batch.size() > 1) {
+            // the merged build failed where each job alone may not: they go
+            // back to the head of the queue and are built one by one
+            std::lock_guard<std::mutex> lk(mu);
+            for (auto it = batch.rbegin(); it != batch.rend(); ++it) {
+                (*it)->state = kQueued;
+                (*it)->solo = true;
+                queue.push_front(*it);
+            }
+            continue;
+        }
         auto hg = std::make_shared<ig::HostGraph>();
         if (s == IG_OK && opts.order_threads == 1) {
             for (size_t b = 0; b < batch.size(); ++b)
@@ -194,6 +275,7 @@ void ig_server::schedule_loop()
             if (s == IG_OK) {
                 pend_g = g;
                 pend_done = done;
+                trim();
                 std::lock_guard<std::mutex> lk(mu);
                 ++batches;
                 max_batch = std::max<int64_t>(max_batch, (int64_t)batch.size());
@@ -205,16 +287,13 @@ void ig_server::schedule_loop()
             s = ig::download_for_greedy(g, opts.order_threads, *hg);
             ig_graph_free(g);
         }
+        trim();
         std::unique_lock<std::mutex> lk(mu);
         ++batches;
         max_batch = std::max<int64_t>(max_batch, (int64_t)batch.size());
         if (s != IG_OK) {
-            for (auto &j : batch) {
-                j->state = kFailed;
-                j->status = s;
-                j->t_done = Clock::now();
-                ++failed;
-            }
+            for (auto &j : batch)
+                fail_job(j, s);
             cv_done.notify_all();
             continue;
         }
@@ -225,6 +304,17 @@ void ig_server::schedule_loop()
         }
         cv_tasks.notify_all();
     }
+}
+
+// After a batch: the context's pair-pass workspaces (grown to the largest
+// batch so far) go back to the device pool when they hold more than a quarter
+// of the HBM budget, so that one dense job does not keep its record buffer
+// for the rest of the stream.
+void ig_server::trim()
+{
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ig::DeviceGuard dg(ctx->device);
+    ig::trim_workspaces(ctx, (size_t)(opts.hbm_budget_bytes / 4));
 }
 
 void ig_server::greedy_loop()
@@ -299,7 +389,7 @@ ig_status ig_server_create(ig_ctx *ctx, const ig_server_opts *opts, ig_server **
         cudaGetLastError();
         if (prev >= 0)
             cudaSetDevice(prev);
-        o.hbm_budget_bytes = (int64_t)(free_b / 2);
+        o.hbm_budget_bytes = (int64_t)(free_b / 10 * 8);
     }
     if (o.pool_reserve_bytes == 0)
         o.pool_reserve_bytes = std::min<int64_t>((int64_t)4 << 30, o.hbm_budget_bytes / 4);
@@ -334,7 +424,6 @@ ig_status ig_server_submit(ig_server *sv, const uint32_t *words, int32_t n, int 
     j->len = len;
     j->min_ed = min_ed;
     j->pairs = (long double)n * (n > 0 ? n - 1 : 0) / 2;
-    j->footprint = footprint_estimate(n, len, min_ed);
     j->t_submit = Clock::now();
     std::unique_lock<std::mutex> lk(sv->mu);
     if (sv->stopping)

@@ -113,6 +113,24 @@ class Context:
               self.handle)
         return int(b.value), int(r.value)
 
+    @property
+    def device_allocs(self) -> int:
+        """Device allocations this context has asked for so far."""
+        k = ctypes.c_int64()
+        check(lib().ig_ctx_alloc_stats(self.handle, ctypes.byref(k)), "ig_ctx_alloc_stats")
+        return int(k.value)
+
+    def set_host_budget(self, nbytes: int):
+        """Host memory downloaded graphs may hold at once (0 = half of RAM)."""
+        check(lib().ig_ctx_set_host_budget(self.handle, int(nbytes)), "ig_ctx_set_host_budget", self.handle)
+
+    def host_budget(self):
+        """(limit, bytes held now) of the host budget."""
+        lim = ctypes.c_int64()
+        used = ctypes.c_int64()
+        check(lib().ig_ctx_host_budget(self.handle, ctypes.byref(lim), ctypes.byref(used)), "ig_ctx_host_budget")
+        return int(lim.value), int(used.value)
+
     def set_wait_limit(self, cycles: int):
         """Bound on the pair kernels' device waits (SM cycles; 0 = default)."""
         check(lib().ig_ctx_set_wait_limit(self.handle, int(cycles)), "ig_ctx_set_wait_limit", self.handle)

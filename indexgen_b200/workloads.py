@@ -111,21 +111,57 @@ def from_strings(strings) -> np.ndarray:
     return pack_digits(raw - 48)
 
 
-def filter_words(words, L: int, max_run: int = 3, min_gc: float = 0.3, max_gc: float = 0.7) -> np.ndarray:
-    """Boolean keep-mask with the reference filter semantics."""
-    d = unpack_digits(words, L).astype(np.int64)
-    keep = np.ones(len(d), bool)
-    if max_run > 0:
-        run = np.ones(len(d), np.int64)
-        best = np.ones(len(d), np.int64)
-        for p in range(1, L):
-            same = d[:, p] == d[:, p - 1]
-            run = np.where(same, run + 1, 1)
+_CHUNK_TABLES = {}
+
+
+def _chunk_tables(k: int):
+    """Per 16-bit chunk value (8 chars at bits 2i) restricted to its first k
+    chars: longest run, leading run, trailing run, first and last char and
+    the count of chars in {1, 2} (C or G)."""
+    t = _CHUNK_TABLES.get(k)
+    if t is None:
+        v = np.arange(1 << 16, dtype=np.uint32)
+        c = ((v[:, None] >> (2 * np.arange(k, dtype=np.uint32))[None, :]) & 3).astype(np.int8)
+        run = np.ones(len(v), np.int8)
+        best = np.ones(len(v), np.int8)
+        lead = np.ones(len(v), np.int8)
+        still = np.ones(len(v), bool)
+        for p in range(1, k):
+            same = c[:, p] == c[:, p - 1]
+            run = np.where(same, run + 1, 1).astype(np.int8)
             best = np.maximum(best, run)
+            still &= same
+            lead = np.where(still, lead + 1, lead).astype(np.int8)
+        gc = ((c == 1) | (c == 2)).sum(axis=1).astype(np.int8)
+        t = (best, lead, run, c[:, 0].copy(), c[:, k - 1].copy(), gc)
+        _CHUNK_TABLES[k] = t
+    return t
+
+
+def filter_words(words, L: int, max_run: int = 3, min_gc: float = 0.3, max_gc: float = 0.7) -> np.ndarray:
+    """Boolean keep-mask with the reference filter semantics (MaxRun <= maxRun
+    when maxRun > 0; GC fraction compared in double when either bound is set),
+    evaluated with per-8-character lookup tables."""
+    w = np.asarray(words, dtype=np.uint32)
+    keep = np.ones(len(w), bool)
+    if len(w) == 0:
+        return keep
+    lo = w & np.uint32(0xffff)
+    k_lo = min(L, 8)
+    b0, _, t0, _, last0, g0 = _chunk_tables(k_lo)
+    best = b0[lo].astype(np.int64)
+    gc = g0[lo].astype(np.int64)
+    if L > 8:
+        hi = (w >> np.uint32(16)) & np.uint32(0xffff)
+        b1, l1, _, first1, _, g1 = _chunk_tables(L - 8)
+        join = np.where(last0[lo] == first1[hi], t0[lo].astype(np.int64) + l1[hi], 0)
+        best = np.maximum(np.maximum(best, b1[hi]), join)
+        gc += g1[hi]
+    if max_run > 0:
         keep &= best <= max_run
     if min_gc > 0 or max_gc > 0:
-        gc = ((d == 1) | (d == 2)).sum(axis=1).astype(np.float64) / float(L)
-        keep &= (gc >= min_gc) & (gc <= max_gc)
+        frac = gc.astype(np.float64) / float(L)
+        keep &= (frac >= min_gc) & (frac <= max_gc)
     return keep
 
 
@@ -265,12 +301,10 @@ def clustered14(total: int = 1_000_000, k: int = 64, seed: int = 14):
     return [w[p] for p in parts]
 
 
-def serving_stream(jobs: int, seed: int, rate: float = 50.0, nmin: int = 5000, nmax: int = 500000,
-                   lengths=(10, 16), dists=(3, 5)):
-    """Seeded stream of codebook jobs: Poisson arrivals (mean `rate` jobs/s),
-    n uniform in [lengths], editDist uniform in [dists], candidate count
-    log-uniform in [nmin, nmax] (counted after the maxRun 3 / GC [0.3,0.7]
-    filters).  Returns a list of (arrival_s, words, n, editDist)."""
+def serving_stream_specs(jobs: int, seed: int, rate: float = 50.0, nmin: int = 5000, nmax: int = 500000,
+                         lengths=(10, 16), dists=(3, 5)):
+    """The jobs of serving_stream without their words: (arrival_s, count, n,
+    editDist, word seed) each; serving_job_words(spec) draws the words."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -279,6 +313,21 @@ def serving_stream(jobs: int, seed: int, rate: float = 50.0, nmin: int = 5000, n
         L = int(rng.integers(lengths[0], lengths[1] + 1))
         d = int(rng.integers(dists[0], dists[1] + 1))
         count = int(round(float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))))
-        words = uniform_until(count, L, int(rng.integers(1 << 31)), max_run=3, min_gc=0.3, max_gc=0.7)
-        out.append((t, words, L, d))
+        out.append((t, count, L, d, int(rng.integers(1 << 31))))
     return out
+
+
+def serving_job_words(spec) -> np.ndarray:
+    """The filtered words of one serving_stream_specs entry."""
+    _, count, L, _, wseed = spec
+    return uniform_until(count, L, wseed, max_run=3, min_gc=0.3, max_gc=0.7)
+
+
+def serving_stream(jobs: int, seed: int, rate: float = 50.0, nmin: int = 5000, nmax: int = 500000,
+                   lengths=(10, 16), dists=(3, 5)):
+    """Seeded stream of codebook jobs: Poisson arrivals (mean `rate` jobs/s),
+    n uniform in [lengths], editDist uniform in [dists], candidate count
+    log-uniform in [nmin, nmax] (counted after the maxRun 3 / GC [0.3,0.7]
+    filters).  Returns a list of (arrival_s, words, n, editDist)."""
+    return [(t, serving_job_words((t, c, L, d, ws)), L, d)
+            for t, c, L, d, ws in serving_stream_specs(jobs, seed, rate, nmin, nmax, lengths, dists)]

@@ -90,3 +90,65 @@ def test_bad_call_among_concurrent_solves():
             assert results[i][1] == edges and np.array_equal(results[i][0], book)
     finally:
         ctx.close()
+
+
+def test_merged_build_that_fails_is_split_per_request():
+    """Two calls that arrive while a long build holds the device are built
+    together next.  The first device allocation of that merged build is made
+    to fail (as a summed workspace that does not fit would); each request is
+    then built on its own and both callers get their exact codebooks."""
+    import time
+
+    from indexgen_b200 import FAULT_DEVICE_ALLOC, FAULT_NONE, Context, solve, workloads as W
+
+    big = (W.uniform_words(400000, 12, 5), 12, 4)
+    small = [(W.uniform_words(3000, 12, 6), 12, 4), (W.uniform_words(2500, 11, 7), 11, 3)]
+    ref = Context(0)
+    try:
+        ref.set_coalescing(False)
+        want = [solve(w, L, d, 1, ref) for w, L, d in small]
+        # allocations of the big call alone on a fresh context
+        probe = Context(0)
+        try:
+            solve(*big, 1, probe)
+            big_allocs = probe.device_allocs
+        finally:
+            probe.close()
+    finally:
+        ref.close()
+    ctx = Context(0)
+    got = [None, None]
+    errors = []
+
+    def run_big():
+        try:
+            solve(*big, 1, ctx)
+        except Exception as e:
+            errors.append(("big", repr(e)))
+
+    def run_small(i):
+        try:
+            w, L, d = small[i]
+            got[i] = solve(w, L, d, 1, ctx)
+        except Exception as e:
+            errors.append((i, repr(e)))
+
+    try:
+        ctx.inject_fault(FAULT_DEVICE_ALLOC, big_allocs + 1)
+        tb = threading.Thread(target=run_big)
+        tb.start()
+        time.sleep(0.03)  # the big build holds the device for much longer than this
+        ts = [threading.Thread(target=run_small, args=(i,)) for i in range(2)]
+        for t in ts:
+            t.start()
+        for t in [tb] + ts:
+            t.join()
+        ctx.inject_fault(FAULT_NONE)
+        assert not errors, errors
+        for (book, edges), (wbook, wedges) in zip(got, want):
+            assert edges == wedges
+            assert np.array_equal(book, wbook)
+        batches, requests = ctx.coalesce_stats()
+        assert requests == 3 and batches == 2  # the big call, then the two small ones merged
+    finally:
+        ctx.close()

@@ -73,3 +73,56 @@ def test_server_with_threaded_neighbour_order(igctx):
         for tk, (order, edges) in zip(tickets, solo):
             got, e, _ = sv.wait(tk)
             assert e == edges and np.array_equal(got, order)
+
+
+def test_server_rejects_a_job_larger_than_its_hbm_budget(igctx):
+    """With a 64 MB HBM budget, a dense job (20,000 n=10 words, editDist 5:
+    about 9e6 edges, some 200 MB at its peak) is refused with IG_ERR_OOM as
+    soon as its sampled edge count is known; the jobs around it are served
+    and equal their solo solves."""
+    from indexgen_b200 import IndexGenError, Server, solve, workloads as W
+
+    small = [(W.uniform_words(2500 + 300 * i, 12, 40 + i), 12, 4) for i in range(5)]
+    dense = (W.uniform_words(20000, 10, 77), 10, 5)
+    want = [solve(w, L, d, 1, igctx)[0] for w, L, d in small]
+    with Server(igctx, host_threads=2, hbm_budget_bytes=64 << 20) as sv:
+        tk = [sv.submit(w, L, d) for w, L, d in small[:2]]
+        td = sv.submit(*dense)
+        tk += [sv.submit(w, L, d) for w, L, d in small[2:]]
+        with pytest.raises(IndexGenError) as ei:
+            sv.wait(td)
+        assert ei.value.status == 3  # IG_ERR_OOM
+        for t, w in zip(tk, want):
+            got, _, _ = sv.wait(t)
+            assert np.array_equal(got, w)
+        assert sv.stats()["completed"] == len(small)
+
+
+def test_server_estimate_failure_fails_cleanly_and_serves_on(igctx):
+    """The next device allocation is made to fail while jobs wait: the jobs
+    whose admission needed it fail with IG_ERR_OOM, jobs submitted afterwards
+    are served exactly."""
+    import time
+
+    from indexgen_b200 import FAULT_DEVICE_ALLOC, FAULT_NONE, IndexGenError, Server, solve, workloads as W
+
+    jobs = [(W.uniform_words(3000 + 200 * i, 11, 60 + i), 11, 3) for i in range(4)]
+    want = [solve(w, L, d, 1, igctx)[0] for w, L, d in jobs]
+    with Server(igctx, host_threads=2) as sv:
+        first = sv.submit(*jobs[0])
+        sv.wait(first)  # the server is warm and idle
+        igctx.inject_fault(FAULT_DEVICE_ALLOC, 1)
+        t1 = sv.submit(*jobs[1])
+        try:
+            sv.wait(t1)
+            failed = False
+        except IndexGenError as e:
+            assert e.status == 3, str(e)
+            failed = True
+        igctx.inject_fault(FAULT_NONE)
+        assert failed, "the injected allocation failure was not reached"
+        time.sleep(0.01)
+        later = [sv.submit(*j) for j in jobs[2:]]
+        for t, w in zip(later, want[2:]):
+            got, _, _ = sv.wait(t)
+            assert np.array_equal(got, w)
