@@ -205,6 +205,52 @@ def run_reference(args, wl, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_gpu(args, wl, rank):
+    """The reference's own GPU path, unmodified: solve_edit_distance_cuda of
+    src/cuda_edit_distance.py (Numba kernel compute_chunk_kernel, 16,384-square
+    tiles, per-edge Python lists), installed into baseline/_ref/src by
+    oracle/Makefile (target `numba`).  Timed as one call on the whole workload
+    after a warm-up call on its first 2,048 words (which JIT-compiles the
+    kernels); the edge count is reported beside the rate, since the reference
+    drops edges past 5,000,000 per tile (src/cuda_edit_distance.py:401-402)."""
+    if rank != 0:
+        return
+    src = os.path.join(ROOT, "baseline", "_ref", "src")
+    base = {"impl": "reference_gpu", "metric": METRIC, "unit": UNIT, "config": {"workload": wl["name"]}}
+    if not os.path.exists(os.path.join(src, "cuda_edit_distance.py")):
+        print(json.dumps({**base, "unavailable": "baseline/_ref/src holds no reference GPU path "
+                                                  "(make -C oracle numba REF=<reference checkout>)"}), flush=True)
+        return
+    sys.path.insert(0, src)
+    try:
+        import cuda_edit_distance as R  # the reference's module
+    except Exception as e:  # numba or its CUDA binding missing
+        print(json.dumps({**base, "unavailable": f"import failed: {e!r}"[:300]}), flush=True)
+        return
+    L, d = wl["L"], wl["min_ed"]
+    strings = W.to_strings(wl["words"], L)
+    try:
+        t0 = time.perf_counter()
+        R.solve_edit_distance_cuda(strings[:2048], d)
+        t_warm = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        adj = R.solve_edit_distance_cuda(strings, d)
+        secs = time.perf_counter() - t0
+    except Exception as e:
+        print(json.dumps({**base, "unavailable": f"the reference GPU path failed: {e!r}"[:300]}), flush=True)
+        return
+    n = len(strings)
+    edges = sum(len(a) for a in adj) // 2
+    pairs = n * (n - 1) // 2
+    line = {**base, "value": pairs / secs / 1e9, "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": 1e3 * secs,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": wl["name"], "desc": wl["desc"], "n": n, "L": L, "min_ed": d, "pairs_per_step": pairs},
+            "edges": edges, "warmup_call_s": t_warm,
+            "note": "solve_edit_distance_cuda(strings, editDist) with its defaults (tile 16384, 9 GB), wall clock: "
+                    "host preparation, kernels, per-tile 40 MB edge-buffer copies and the per-edge Python lists"}
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------------------------ ours ----
 def profile_traffic(wl_name):
     """dram bytes per pair-kernel launch from the committed ncu summary, if any."""
@@ -344,6 +390,13 @@ def run_batch_section(ctx, reps: int = 6) -> dict:
             "threaded_solve_uncoalesced_jobs_per_s": len(jobs) / t_thr_off,
             "batched_pair_kernel_gpairs_per_s": (pairs / (pair_ms / 1e3) / 1e9) if pair_ms else None,
             "host_threads": cores, "identical_to_plain": bool(same),
+            # the plain loop is one thread; the split below separates what
+            # host threads give from what device batching gives
+            "gain_split": {"host_threading": t_plain / t_thr_off,
+                           "device_batching_vs_uncoalesced_threads": t_thr_off / tb,
+                           "device_batching_vs_coalesced_threads": t_thr / tb,
+                           "note": "plain loop (1 thread) -> 16 threads calling solve one job per launch -> "
+                                   "solve_batch; the factors multiply to speedup_vs_plain"},
             "note": "wall clock through solve_batch vs a loop of solve (graph + greedy per cluster)"}
 
 
@@ -766,6 +819,33 @@ def run_ours(args, wl, rank, world, dist):
             sel = G.codebook(1)
             greedy_ms = 1e3 * (time.perf_counter() - t0)
 
+    # ---- words -> codebook through the public API (host words in, codebook
+    # out), and its parts measured apart on the same context
+    from indexgen_b200 import codebook_from_adjacency, solve
+
+    solve_ms = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        book, _ = solve(words, L, d, 1, ctx)
+        solve_ms.append(1e3 * (time.perf_counter() - t0))
+    t0 = time.perf_counter()
+    G = build_conflict_graph(words, L, d, ctx)
+    t_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ap, adj = G.adjacency()
+    t_adj = time.perf_counter() - t0
+    G.close()
+    t0 = time.perf_counter()
+    book2 = codebook_from_adjacency(ap, adj, n)
+    t_greedy = time.perf_counter() - t0
+    solve_e2e = {"ms": min(solve_ms), "build_from_host_words_ms": 1e3 * t_build,
+                 "adjacency_build_and_download_ms": 1e3 * t_adj, "host_greedy_ms": 1e3 * t_greedy,
+                 "codebook": int(len(book)), "same_codebook_both_ways": bool(np.array_equal(book, book2)),
+                 "h2d_bytes": 4 * n, "d2h_adjacency_bytes": 8 * (n + 1) + 8 * edges,
+                 "note": "solve() = ig_solve(host words) -> codebook, wall clock, best of 3; the parts are separate "
+                         "calls: ig_graph_build, ig_graph_adjacency (device canonical order + pinned download), "
+                         "ig_codebook_from_adjacency (the sequential greedy, one host thread)"}
+
     peaks, src = measured_peaks()
     sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     alu_peak = props.multi_processor_count * 64 * sm_mhz * 1e6 / 1e12  # ALU pipe: 64 lanes/clk/SM
@@ -815,6 +895,7 @@ def run_ours(args, wl, rank, world, dist):
         "cuda_graphs": dict(zip(("launches", "instantiations", "updates"), ctx.graph_stats())),
         "clocks": clk,
         "greedy": {"ms": greedy_ms, "codebook": int(len(sel)), "order_threads": 1, "where": "host C++ (library)"},
+        "solve_e2e": solve_e2e,
     }
     if not args.no_batch:
         line["batch"] = run_batch_section(ctx)
@@ -834,7 +915,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference_gpu"])
     ap.add_argument("--workload", default="linear12", choices=["linear12", "uniform11", "vt16", "serve5"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-clusters section")
@@ -850,7 +931,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.workload == "serve5":
-        if args.impl == "reference" or world > 1:
+        if args.impl != "ours" or world > 1:
             if rank == 0:
                 print(json.dumps({"impl": args.impl, "unavailable": "the config-5 serving stream is a one-GPU "
                                   "comparison of the library's server with its own one-job-per-launch path"}))
@@ -864,6 +945,9 @@ def main():
         wl["name"] += f"_subset{args.subset}"
     if args.impl == "reference":
         run_reference(args, wl, rank)
+        return
+    if args.impl == "reference_gpu":
+        run_reference_gpu(args, wl, rank)
         return
     dist = None
     if world > 1:

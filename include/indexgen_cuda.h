@@ -340,6 +340,12 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
 /* Number of conflicting pairs only (VerifyDist's GPU branch passes when it is
  * zero, src/Utils.cpp:203-288). */
 ig_status ig_count_conflicts(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int min_ed, int64_t *edges);
+/* Greedy over caller-supplied neighbour lists in host memory, taken in the
+ * order given -- AdjList::m as the reference holds it before RowsBySum
+ * (src/SparseMat.cpp:81-120), e.g. the lists of ig_graph_adjacency; each
+ * undirected edge appears in both lists (no device work). */
+ig_status ig_codebook_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order,
+                                     int32_t *count);
 /* Greedy over a caller-supplied upper CSR in host memory (no device work). */
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count);
@@ -357,8 +363,10 @@ ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols
  * scratch is a fixed array inside the library image, at most
  * IG_NOALLOC_MAX_WORDS words per call (larger n: IG_ERR_CAPACITY).  The first
  * call on each device looks up that array's device address; make it before
- * any stream capture.  All calls share the array: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * any stream capture.  The address is kept for the life of the process: a
+ * host that resets a device (cudaDeviceReset) must not call this entry point
+ * on that device again in the same process.  All calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
 #define IG_NOALLOC_MAX_WORDS 65536
 ig_status ig_count_conflicts_noalloc(const uint32_t *words, int32_t n, int len, int min_ed,
                                      unsigned long long *count, void *stream);

@@ -23,6 +23,7 @@ from .graph import (  # noqa: F401
     build_conflict_graph,
     cluster_centres,
     cluster_solve,
+    codebook_from_adjacency,
     codebook_from_upper_csr,
     count_conflicts,
     default_context,

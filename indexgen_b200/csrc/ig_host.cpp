@@ -335,6 +335,28 @@ ig_status ig_filter(const uint32_t *words, int64_t n, int len, int max_run, doub
     IG_ABI_CATCH
 }
 
+ig_status ig_codebook_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int32_t *order,
+                                     int32_t *count)
+{
+    IG_ABI_TRY
+    if (n < 0 || !count || (n > 0 && (!adj_ptr || !order)) || (n > 0 && adj_ptr[n] > 0 && !adj) ||
+        (n > 0 && adj_ptr[0] != 0))
+        return IG_ERR_INPUT;
+    for (int32_t i = 0; i < n; ++i)
+        if (adj_ptr[i + 1] < adj_ptr[i])
+            return IG_ERR_INPUT;
+    for (int64_t k = 0; n > 0 && k < adj_ptr[n]; ++k)
+        if (adj[k] < 0 || adj[k] >= n)
+            return IG_ERR_INPUT;
+    try {
+        *count = ig::greedy_from_adjacency(adj_ptr, adj, n, 0, order);
+    } catch (...) {
+        return IG_ERR_OOM;
+    }
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count)
 {

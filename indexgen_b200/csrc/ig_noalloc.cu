@@ -15,7 +15,9 @@
 // address (there it is only a host-side stand-in): the first call on each
 // device, with that device current, looks the address up once with
 // cudaGetSymbolAddress and caches it.  Make that first call before any stream
-// capture begins.
+// capture begins.  The cache lives as long as the process: after a
+// cudaDeviceReset the module may come back at another address, so a host that
+// resets a device must not call this entry point on it again.
 //
 // Limits and sharing: at most IG_NOALLOC_MAX_WORDS words per call.  Every call
 // uses the same array and leaves its contents behind; each call clears the two

@@ -404,6 +404,18 @@ def assign_centers(words, centers, L: int, ctx: Context | None = None):
     return out[: len(w)]
 
 
+def codebook_from_adjacency(adj_ptr, adj, n: int) -> np.ndarray:
+    """Greedy codebook over host neighbour lists taken in the given order
+    (the reference's AdjList::m, e.g. ConflictGraph.adjacency())."""
+    ap = np.ascontiguousarray(adj_ptr, dtype=np.int64)
+    a = np.ascontiguousarray(adj, dtype=np.int32)
+    order = np.zeros(max(int(n), 1), np.int32)
+    cnt = ctypes.c_int32()
+    check(lib().ig_codebook_from_adjacency(ptr(ap), ptr(a), int(n), ptr(order), ctypes.byref(cnt)),
+          "ig_codebook_from_adjacency")
+    return order[: cnt.value].copy()
+
+
 def codebook_from_upper_csr(row_ptr, cols, n: int, order_threads: int = 1) -> np.ndarray:
     rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
     cl = np.ascontiguousarray(cols, dtype=np.int32)
@@ -654,7 +666,7 @@ def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
 __all__ = [
     "Context", "ConflictGraph", "IndexGenError", "Server", "FAULT_NONE", "FAULT_DEVICE_ALLOC", "FAULT_TILE_COPY", "build_conflict_graph", "build_batch", "solve_batch",
     "count_conflicts",
-    "codebook_from_upper_csr", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
+    "codebook_from_upper_csr", "codebook_from_adjacency", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
     "solve_assignments_cuda", "random_cluster_fit", "cluster_solve", "cluster_centres", "read_adj_list",
 ]

@@ -106,6 +106,21 @@ def test_host_greedy_small_cases(L):
         assert np.array_equal(codebook_from_upper_csr(row_ptr, cols, n, 3), g[key + "_sel3"]), key
 
 
+def test_host_greedy_over_reference_neighbour_lists(L):
+    """Greedy over neighbour lists as the reference's AdjList holds them: the
+    reference's own m[] at T=3 (small_cases.npz) gives its T=3 codebooks."""
+    from indexgen_b200 import IndexGenError, codebook_from_adjacency
+
+    g = load_golden("small_cases.npz")
+    keys = sorted({k.rsplit("_", 1)[0] for k in g.files if k.endswith("_words")})
+    for key in keys:
+        n = len(g[key + "_words"])
+        assert np.array_equal(codebook_from_adjacency(g[key + "_adj3_ptr"], g[key + "_adj3"], n),
+                              g[key + "_sel3"]), key
+    with pytest.raises(IndexGenError):
+        codebook_from_adjacency(np.array([0, 1, 1], np.int64), np.array([4], np.int32), 2)
+
+
 def test_host_greedy_rejects_bad_csr(L):
     from indexgen_b200 import IndexGenError, codebook_from_upper_csr
 
