@@ -129,6 +129,19 @@ ig_status ig_ctx_set_wait_limit(ig_ctx *ctx, int64_t cycles);
  *   IG_FAULT_TILE_COPY     the next pair pass does not issue the copy of the
  *                          first staged tile of each pair kernel's first work
  *                          item, so that tile's bounded wait runs out. */
+/* Form of the neighbour lists a graph is sent in to the host greedy:
+ *   IG_LISTS_AUTO    packed when the plain lists would take 512 MB or more
+ *                    (the default);
+ *   IG_LISTS_PLAIN   offsets and 4-byte neighbour ids;
+ *   IG_LISTS_PACKED  each row bit-packed on the device (gap width, first
+ *                    neighbour, gaps in that width): 2-3x less PCIe traffic
+ *                    and host memory per graph, about 1 ns more greedy time
+ *                    per neighbour.
+ * The codebooks do not depend on it. */
+#define IG_LISTS_AUTO 0
+#define IG_LISTS_PLAIN 1
+#define IG_LISTS_PACKED 2
+ig_status ig_ctx_set_host_lists(ig_ctx *ctx, int form);
 /* Device allocations this context has asked for so far (workspaces grow
  * rarely and are reused, so a steady stream of builds adds only the graphs'
  * own arrays); with IG_FAULT_DEVICE_ALLOC it tells a test which one to fail. */

@@ -16,6 +16,9 @@ from .graph import (  # noqa: F401
     LANES_BYTE,
     LANES_FULL,
     LANES_NIBBLE,
+    LISTS_AUTO,
+    LISTS_PACKED,
+    LISTS_PLAIN,
     Server,
     apply_filters,
     assign_centers,

@@ -26,7 +26,7 @@ EXPORTS = (
     "ig_server_stats", "ig_server_destroy",
     "ig_lane_form", "ig_ctx_autotune", "ig_ctx_set_work_split", "ig_ctx_work_split", "ig_ctx_set_autotune",
     "ig_ctx_set_graphs", "ig_ctx_graph_stats", "ig_ctx_set_coalescing", "ig_ctx_coalesce_stats",
-    "ig_ctx_set_wait_limit", "ig_ctx_inject_fault", "ig_ctx_set_host_budget", "ig_ctx_host_budget", "ig_ctx_alloc_stats",
+    "ig_ctx_set_wait_limit", "ig_ctx_inject_fault", "ig_ctx_set_host_budget", "ig_ctx_host_budget", "ig_ctx_alloc_stats", "ig_ctx_set_host_lists",
 )
 
 STATUS = {0: "IG_OK", 1: "IG_ERR_INPUT", 2: "IG_ERR_CAPACITY", 3: "IG_ERR_OOM", 4: "IG_ERR_CUDA",
@@ -115,6 +115,7 @@ def _declare(L):
         "ig_ctx_set_wait_limit": (_int, [_vp, _i64]),
         "ig_ctx_set_host_budget": (_int, [_vp, _i64]),
         "ig_ctx_alloc_stats": (_int, [_vp, ctypes.POINTER(_i64)]),
+        "ig_ctx_set_host_lists": (_int, [_vp, _int]),
         "ig_ctx_host_budget": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
         "ig_ctx_inject_fault": (_int, [_vp, _int, _i64]),
         "ig_ctx_coalesce_stats": (_int, [_vp, ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),

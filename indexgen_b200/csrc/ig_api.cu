@@ -139,6 +139,10 @@ void release_graph(ig_graph *g, bool caller_holds_lock = false)
             cudaFreeAsync(g->d_adj_ptr, g->ctx->stream);
         if (g->d_adj)
             cudaFreeAsync(g->d_adj, g->ctx->stream);
+        if (g->d_pk_off)
+            cudaFreeAsync(g->d_pk_off, g->ctx->stream);
+        if (g->d_pk)
+            cudaFreeAsync(g->d_pk, g->ctx->stream);
         cudaStreamSynchronize(g->ctx->stream);
     }
     delete g;
@@ -189,40 +193,110 @@ std::shared_ptr<void> host_block(Ctx *ctx, size_t bytes, std::shared_ptr<void> t
     });
 }
 
-size_t adjacency_host_bytes(const Graph *g)
+// A graph goes to the host greedy as its canonical adjacency (offsets and
+// 4-byte neighbour ids) or, when that would take at least kPackRowsMinBytes,
+// with its rows bit-packed (ig_packrows.cu): the packing cuts the copy and
+// the host memory a dense graph holds while its greedy runs by 2-3x, and the
+// decoding adds about 1 ns per neighbour to the greedy, which a small graph's
+// download does not win back.
+constexpr size_t kPackRowsMinBytes = (size_t)512 << 20;
+
+bool pack_for_host(const Graph *g)
 {
-    return ((size_t)g->n + 1) * sizeof(int64_t) + (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
+    const int form = g->ctx->host_lists.load();
+    if (form != IG_LISTS_AUTO)
+        return form == IG_LISTS_PACKED;
+    return ((size_t)g->n + 1) * sizeof(int64_t) + (size_t)g->edges * 8 >= kPackRowsMinBytes;
 }
 
-// Canonical symmetric adjacency on the device (built once), then into one
-// host block: offsets first, then neighbours.
+// Host bytes of a graph's download for the greedy.
+size_t download_bytes(const Graph *g, bool packed)
+{
+    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
+    if (packed)
+        return 2 * ptr_bytes + ((size_t)g->pk_words + 2) * sizeof(uint32_t);
+    return ptr_bytes + (size_t)std::max<int64_t>(2 * g->edges, 1) * sizeof(int32_t);
+}
+
+// Decides the download's form and takes its share of the host budget with the
+// context lock released, so that a caller whose greedy would free host room is
+// never kept waiting for the device.  Packed rows are built first (their size
+// is known only then); the plain adjacency is built by the copy.
+ig_status reserve_download(ig_graph *g, bool &packed, std::shared_ptr<void> &token)
+{
+    ig::Ctx *ctx = g->ctx;
+    packed = pack_for_host(g);
+    if (packed) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        DeviceGuard dg(ctx->device);
+        ig_status s = build_packed_rows(ctx, g);
+        if (s != IG_OK)
+            return s;
+    }
+    token = ctx->host_budget->acquire((int64_t)download_bytes(g, packed));
+    return IG_OK;
+}
+
+// Caller holds ctx->mu: the graph's greedy form into one new host block,
+// copied on `st`.
+ig_status queue_download(ig_graph *g, bool packed, std::shared_ptr<void> token, cudaStream_t st, HostGraph &hg)
+{
+    ig::Ctx *ctx = g->ctx;
+    if (!packed) {
+        ig_status s = build_adjacency(ctx, g);  // ends with the context stream idle
+        if (s != IG_OK)
+            return s;
+    }
+    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
+    std::shared_ptr<void> block = host_block(ctx, download_bytes(g, packed), std::move(token));
+    if (!block)
+        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
+    char *base = static_cast<char *>(block.get());
+    int64_t *ap = reinterpret_cast<int64_t *>(base);
+    cudaError_t e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, st);
+    hg.ptr = ap;
+    if (packed) {
+        int64_t *po = reinterpret_cast<int64_t *>(base + ptr_bytes);
+        uint32_t *pk = reinterpret_cast<uint32_t *>(base + 2 * ptr_bytes);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(po, g->d_pk_off, ptr_bytes, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(pk, g->d_pk, ((size_t)g->pk_words + 2) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        hg.idx = nullptr;
+        hg.pk_off = po;
+        hg.pk = pk;
+    } else {
+        int32_t *adj = reinterpret_cast<int32_t *>(base + ptr_bytes);
+        if (e == cudaSuccess && g->edges > 0)
+            e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        hg.idx = adj;
+        hg.pk_off = nullptr;
+        hg.pk = nullptr;
+    }
+    hg.storage = std::move(block);
+    if (e != cudaSuccess) {
+        cudaStreamSynchronize(st);
+        hg.storage.reset();
+        return cuda_error(ctx, e, "adjacency download");
+    }
+    return IG_OK;
+}
+
+// The graph's greedy form on the host (blocking).
 ig_status fetch_adjacency(ig_graph *g, HostGraph &hg)
 {
     ig::Ctx *ctx = g->ctx;
-    std::shared_ptr<void> token = ctx->host_budget->acquire((int64_t)adjacency_host_bytes(g));
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    DeviceGuard dg(ctx->device);
-    ig_status s = build_adjacency(ctx, g);
+    bool packed = false;
+    std::shared_ptr<void> token;
+    ig_status s = reserve_download(g, packed, token);
     if (s != IG_OK)
         return s;
-    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
-    std::shared_ptr<void> block = host_block(ctx, adjacency_host_bytes(g), std::move(token));
-    if (!block)
-        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
-    int64_t *ap = static_cast<int64_t *>(block.get());
-    int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
-    cudaError_t e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess && g->edges > 0)
-        e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                            ctx->stream);
-    if (e == cudaSuccess)
-        e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess)
-        return cuda_error(ctx, e, "adjacency download");
-    hg.ptr = ap;
-    hg.idx = adj;
-    hg.storage = std::move(block);
-    return IG_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
+    if ((s = queue_download(g, packed, std::move(token), ctx->stream, hg)) != IG_OK)
+        return s;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    return e == cudaSuccess ? IG_OK : cuda_error(ctx, e, "adjacency download");
 }
 
 // Validated job list from an offsets array.
@@ -256,41 +330,28 @@ ig_status make_jobs(Ctx *ctx, const int64_t *offsets, int32_t k, const int32_t *
 ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, cudaHostFn_t then, void *arg)
 {
     ig::Ctx *ctx = g->ctx;
-    std::shared_ptr<void> token = ctx->host_budget->acquire((int64_t)adjacency_host_bytes(g));
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    DeviceGuard dg(ctx->device);
-    ig_status s = build_adjacency(ctx, g);  // ends with the context stream idle
+    bool packed = false;
+    std::shared_ptr<void> token;
+    ig_status s = reserve_download(g, packed, token);
     if (s != IG_OK)
         return s;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    DeviceGuard dg(ctx->device);
     cudaError_t e = cudaSuccess;
     if (!ctx->dl_stream && (e = cudaStreamCreateWithFlags(&ctx->dl_stream, cudaStreamNonBlocking)) != cudaSuccess) {
         ctx->dl_stream = nullptr;
         return cuda_error(ctx, e, "download stream");
     }
-    const size_t ptr_bytes = ((size_t)g->n + 1) * sizeof(int64_t);
-    std::shared_ptr<void> block = host_block(ctx, adjacency_host_bytes(g), std::move(token));
-    if (!block)
-        return set_error(ctx, IG_ERR_OOM, "host adjacency allocation failed");
-    int64_t *ap = static_cast<int64_t *>(block.get());
-    int32_t *adj = reinterpret_cast<int32_t *>(static_cast<char *>(block.get()) + ptr_bytes);
     cudaEvent_t fin = nullptr;
     if ((e = cudaEventCreateWithFlags(&fin, cudaEventDisableTiming)) != cudaSuccess)
         return cuda_error(ctx, e, "download event");
-    e = cudaMemcpyAsync(ap, g->d_adj_ptr, ptr_bytes, cudaMemcpyDeviceToHost, ctx->dl_stream);
-    if (e == cudaSuccess && g->edges > 0)
-        e = cudaMemcpyAsync(adj, g->d_adj, (size_t)(2 * g->edges) * sizeof(int32_t), cudaMemcpyDeviceToHost,
-                            ctx->dl_stream);
-    if (e != cudaSuccess) {
-        cudaStreamSynchronize(ctx->dl_stream);
-        cudaEventDestroy(fin);
-        return cuda_error(ctx, e, "adjacency download");
-    }
     hg.order_threads = 1;
     hg.jobs = g->jobs;
     hg.job_edge_off = g->job_edge_off;
-    hg.ptr = ap;
-    hg.idx = adj;
-    hg.storage = std::move(block);
+    if ((s = queue_download(g, packed, std::move(token), ctx->dl_stream, hg)) != IG_OK) {
+        cudaEventDestroy(fin);
+        return s;
+    }
     if (then && (e = cudaLaunchHostFunc(ctx->dl_stream, then, arg)) != cudaSuccess) {
         cudaStreamSynchronize(ctx->dl_stream);
         cudaEventDestroy(fin);
@@ -323,18 +384,31 @@ bool reserve_pool(Ctx *ctx, size_t bytes)
 
 std::shared_ptr<void> PinnedPool::acquire(size_t bytes)
 {
+    // size classes: powers of two up to 1 GiB, whole GiB above
+    constexpr size_t kGiB = (size_t)1 << 30;
     size_t cls = (size_t)1 << 20;
-    while (cls < bytes)
+    while (cls < bytes && cls < kGiB)
         cls <<= 1;
+    if (cls < bytes)
+        cls = (bytes + kGiB - 1) / kGiB * kGiB;
+    const size_t slack = cls < kGiB ? 3 * cls : 2 * kGiB;  // a cached block this much larger still serves
     void *p = nullptr;
     {
         std::lock_guard<std::mutex> lk(mu_);
         auto it = free_.lower_bound(cls);
-        if (it != free_.end() && it->first <= 4 * cls) {
+        if (it != free_.end() && it->first <= cls + slack) {
             cls = it->first;
             p = it->second;
             free_.erase(it);
         } else {
+            // make room by unpinning cached blocks that serve no one now
+            while (total_ + cls > kCap && !free_.empty()) {
+                auto big = std::prev(free_.end());
+                cudaFreeHost(big->second);
+                total_ -= big->first;
+                free_.erase(big);
+            }
+            cudaGetLastError();
             if (total_ + cls > kCap)
                 return nullptr;
             total_ += cls;  // reserved before the (slow) pinning, outside the lock
@@ -395,6 +469,8 @@ ig_status download_for_greedy(Graph *gg, int order_threads, HostGraph &hg)
 int32_t greedy_one(const HostGraph &hg, int job, int32_t *out)
 {
     const JobSpec &J = hg.jobs[(size_t)job];
+    if (hg.pk)
+        return greedy_from_packed(hg.ptr + J.word_off, hg.pk_off + J.word_off, hg.pk, J.n, J.word_off, out);
     if (hg.order_threads == 1)
         return greedy_from_adjacency(hg.ptr + J.word_off, hg.idx, J.n, J.word_off, out);
     return greedy_from_upper(hg.ptr + J.word_off, hg.idx, J.n, J.word_off, hg.order_threads, out);
@@ -1374,19 +1450,23 @@ ig_status ig_solve(ig_ctx *ctx, const uint32_t *words, int32_t n, int len, int m
         *count = ig::greedy_one(*req.hg, req.job, order);
         return IG_OK;
     }
-    ig_graph *g = nullptr;
-    ig_status s = ig_graph_build(ctx, words, n, len, min_ed, 0, &g);
-    if (s != IG_OK)
-        return s;
-    if (edges)
-        *edges = g->edges;
-    // the device graph goes before the greedy runs: concurrent callers then
-    // hold host copies only, within the context's host budget
+    // one caller at a time from its build until its device graph is freed;
+    // the greedy runs after that, so concurrent callers hold host copies
+    // only, within the context's host budget
     ig::HostGraph hg;
-    s = ig::download_for_greedy(g, order_threads, hg);
-    ig::release_graph(g);
-    if (s != IG_OK)
-        return s;
+    {
+        std::lock_guard<std::mutex> slot(ctx->solve_slot);
+        ig_graph *g = nullptr;
+        ig_status s = ig_graph_build(ctx, words, n, len, min_ed, 0, &g);
+        if (s != IG_OK)
+            return s;
+        if (edges)
+            *edges = g->edges;
+        s = ig::download_for_greedy(g, order_threads, hg);
+        ig::release_graph(g);
+        if (s != IG_OK)
+            return s;
+    }
     *count = ig::greedy_one(hg, 0, order);
     return IG_OK;
     IG_ABI_CATCH
@@ -1487,6 +1567,16 @@ ig_status ig_ctx_graph_stats(const ig_ctx *ctx, int64_t *launches, int64_t *inst
         *instantiations = ctx->graph_instantiations;
     if (updates)
         *updates = ctx->graph_updates;
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_ctx_set_host_lists(ig_ctx *ctx, int form)
+{
+    IG_ABI_TRY
+    if (!ctx || (form != IG_LISTS_AUTO && form != IG_LISTS_PLAIN && form != IG_LISTS_PACKED))
+        return IG_ERR_INPUT;
+    ctx->host_lists = form;
     return IG_OK;
     IG_ABI_CATCH
 }

@@ -101,12 +101,52 @@ void assemble(const int64_t *row_ptr, const int32_t *cols_in, int32_t n, int64_t
 // #{v : initial degree >= b} slots, which bounds its size at any time because
 // degrees only fall.  The slice array is left uninitialised so only the slots
 // actually used are ever touched.
+// Neighbour lists as the canonical adjacency in memory: row i is a slice of adj.
+struct PlainRows {
+    const int64_t *ap;
+    const int32_t *adj;
+    const int32_t *get(int32_t i, int32_t *) const { return adj + ap[i]; }
+    void prefetch(int32_t i) const { __builtin_prefetch(adj + ap[i]); }
+};
+
+// Neighbour lists bit-packed per row (ig_packrows.cu): a header word with the
+// gap width w, the first neighbour, then the gaps a[k] - a[k-1] - 1 in w bits
+// each; decoded into the caller's buffer just before the row is walked.
+struct PackedRows {
+    const int64_t *ap;   // degrees: ap[i+1] - ap[i]
+    const int64_t *off;  // first word of each row
+    const uint32_t *pk;  // the words (two spare words at the end)
+    const int32_t *get(int32_t i, int32_t *buf) const
+    {
+        const int64_t d = ap[i + 1] - ap[i];
+        if (d == 0)
+            return buf;
+        const uint32_t *row = pk + off[i];
+        const uint32_t w = row[0];
+        const uint32_t *g = row + 2;
+        const uint64_t mask = w >= 32 ? 0xffffffffull : ((1ull << w) - 1);
+        int32_t a = (int32_t)row[1];
+        buf[0] = a;
+        uint64_t pos = 0;
+        for (int64_t k = 1; k < d; ++k, pos += w) {
+            const uint64_t word = pos >> 5;
+            uint64_t v;
+            std::memcpy(&v, g + word, sizeof(v));
+            a += (int32_t)((v >> (pos & 31)) & mask) + 1;
+            buf[k] = a;
+        }
+        return buf;
+    }
+    void prefetch(int32_t i) const { __builtin_prefetch(pk + off[i]); }
+};
+
+template <class Rows>
 class BucketGreedy {
   public:
-    // ap covers the n job rows (its values index adj); neighbour ids in adj
-    // are global and `base` maps them to job-local ids.
-    BucketGreedy(const int64_t *ap, const int32_t *adj, int32_t n, int64_t base)
-        : ap_(ap), adj_(adj), base_(base), v_((size_t)n)
+    // ap covers the n job rows (its differences are the degrees); neighbour
+    // ids in the rows are global and `base` maps them to job-local ids.
+    BucketGreedy(const int64_t *ap, Rows rows, int32_t n, int64_t base)
+        : ap_(ap), rows_(rows), base_(base), v_((size_t)n)
     {
         int32_t maxd = 0;
         for (int32_t i = 0; i < n; ++i) {
@@ -137,6 +177,8 @@ class BucketGreedy {
         }
         active_ = n;
         todel_.reserve((size_t)maxd + 1);
+        bufx_.resize((size_t)maxd + 1);
+        bufi_.resize((size_t)maxd + 1);
     }
 
     int32_t run(int32_t *order)
@@ -147,11 +189,12 @@ class BucketGreedy {
             const int32_t x = data_[(size_t)(start_[(size_t)tracker_] + size_[(size_t)tracker_] - 1)];
             order[cnt++] = x;
             // DelBall: active neighbours in m-order, then the vertex itself
-            const int64_t b = ap_[x], e = ap_[x + 1];
-            todel_.resize((size_t)(e - b) + 1);
+            const int32_t *row = rows_.get(x, bufx_.data());
+            const int64_t len = ap_[x + 1] - ap_[x];
+            todel_.resize((size_t)len + 1);
             int32_t nt = 0;
-            for (int64_t k = b; k < e; ++k) {  // branch-free compaction
-                const int32_t j = (int32_t)(adj_[k] - base_);
+            for (int64_t k = 0; k < len; ++k) {  // branch-free compaction
+                const int32_t j = (int32_t)(row[k] - base_);
                 todel_[(size_t)nt] = j;
                 nt += v_[(size_t)j].deg >= 0;
             }
@@ -159,10 +202,10 @@ class BucketGreedy {
             // the neighbour lists of the ball's vertices are read next: fetch
             // their heads a few vertices ahead
             for (int32_t t = 0; t < nt && t < 4; ++t)
-                __builtin_prefetch(adj_ + ap_[todel_[(size_t)t]]);
+                rows_.prefetch(todel_[(size_t)t]);
             for (int32_t t = 0; t < nt; ++t) {
                 if (t + 4 < nt)
-                    __builtin_prefetch(adj_ + ap_[todel_[(size_t)t + 4]]);
+                    rows_.prefetch(todel_[(size_t)t + 4]);
                 del_row_col(todel_[(size_t)t]);
             }
         }
@@ -204,15 +247,16 @@ class BucketGreedy {
         const int32_t di = v_[(size_t)i].deg;
         if (di < 0)
             return;
-        const int64_t e = ap_[i + 1];
-        for (int64_t k = ap_[i]; k < e; k += 8) {
+        const int32_t *row = rows_.get(i, bufi_.data());
+        const int64_t e = ap_[i + 1] - ap_[i];
+        for (int64_t k = 0; k < e; k += 8) {
             const int m = (int)std::min<int64_t>(8, e - k);
             for (int64_t q = k + 8; q < std::min<int64_t>(k + 16, e); ++q)  // next block's degrees
-                __builtin_prefetch(&v_[(size_t)(adj_[q] - base_)]);
+                __builtin_prefetch(&v_[(size_t)(row[q] - base_)]);
             int32_t jj[8], dd[8];
             unsigned live = 0;
             for (int t = 0; t < m; ++t) {
-                jj[t] = (int32_t)(adj_[k + t] - base_);
+                jj[t] = (int32_t)(row[k + t] - base_);
                 dd[t] = v_[(size_t)jj[t]].deg;
             }
             for (int t = 0; t < m; ++t)
@@ -233,13 +277,13 @@ class BucketGreedy {
         int32_t pos;  // slot inside its degree bucket
     };
     const int64_t *ap_;
-    const int32_t *adj_;
+    Rows rows_;
     int64_t base_;
     std::vector<Vtx> v_;
     std::vector<int32_t> size_;
     std::vector<int64_t> start_;
     std::unique_ptr<int32_t[]> data_;
-    std::vector<int32_t> todel_;
+    std::vector<int32_t> todel_, bufx_, bufi_;
     int32_t nb_ = 0;
     int32_t tracker_ = 0;
     int32_t active_ = 0;
@@ -255,7 +299,7 @@ int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n
     std::vector<int64_t> ap;
     std::vector<int32_t> adj;
     assemble(row_ptr, cols, n, base, order_threads, ap, adj);
-    BucketGreedy g(ap.data(), adj.data(), n, 0);
+    BucketGreedy<PlainRows> g(ap.data(), PlainRows{ap.data(), adj.data()}, n, 0);
     return g.run(order);
 }
 
@@ -263,7 +307,16 @@ int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_
 {
     if (n <= 0)
         return 0;
-    BucketGreedy g(adj_ptr, adj, n, base);
+    BucketGreedy<PlainRows> g(adj_ptr, PlainRows{adj_ptr, adj}, n, base);
+    return g.run(order);
+}
+
+int32_t greedy_from_packed(const int64_t *adj_ptr, const int64_t *pk_off, const uint32_t *pk, int32_t n, int64_t base,
+                           int32_t *order)
+{
+    if (n <= 0)
+        return 0;
+    BucketGreedy<PackedRows> g(adj_ptr, PackedRows{adj_ptr, pk_off, pk}, n, base);
     return g.run(order);
 }
 

@@ -85,11 +85,12 @@ struct DevBuf {
 // Page-locked host blocks for graph downloads, recycled across calls: a
 // pageable download of a few hundred MB runs at a few GB/s and first touches
 // fresh pages, a pinned one at tens of GB/s.  Blocks come in power-of-two
-// sizes; the pool holds at most kCap bytes and callers fall back to pageable
-// memory beyond that (ig_api.cu).
+// sizes up to 1 GiB and whole GiB above; the pool holds at most kCap bytes,
+// unpins cached blocks that no download holds to make room for a new size,
+// and callers fall back to pageable memory beyond that (ig_api.cu).
 class PinnedPool : public std::enable_shared_from_this<PinnedPool> {
 public:
-    static constexpr size_t kCap = (size_t)16 << 30;
+    static constexpr size_t kCap = (size_t)32 << 30;
     // A block of at least `bytes`, returned to the pool when the last copy of
     // the pointer goes; nullptr when the pool is full or pinning fails.
     std::shared_ptr<void> acquire(size_t bytes);
@@ -166,6 +167,11 @@ struct Ctx {
     std::shared_ptr<class GreedyPool> greedy_pool;
     // concurrent ig_solve calls built together (ig_api.cu)
     std::atomic<bool> coalesce{true};
+    // uncoalesced ig_solve calls hold this from their build until their device
+    // graph is freed: callers waiting for host room never hold device graphs
+    std::mutex solve_slot;
+    // form of the neighbour lists sent to the host greedy (IG_LISTS_*)
+    std::atomic<int> host_lists{IG_LISTS_AUTO};
     std::shared_ptr<struct SolveCombiner> combiner;
     // page-locked staging of the graphs' host copies
     void *stage = nullptr;
@@ -208,6 +214,10 @@ struct Graph {
     // symmetric adjacency in canonical order (built on first request)
     int64_t *d_adj_ptr = nullptr;  // [n+1]
     int32_t *d_adj = nullptr;      // [2*edges]
+    // that adjacency bit-packed per row for the host (built on first request)
+    int64_t *d_pk_off = nullptr;   // [n+1] first word of each row
+    uint32_t *d_pk = nullptr;      // [pk_words + 2]
+    int64_t pk_words = 0;
 };
 
 // Geometry of the upper-triangle work decomposition for one job.
@@ -247,6 +257,9 @@ ig_status ensure_buffer(Ctx *ctx, DevBuf &b, size_t bytes, const char *what);
 bool reserve_pool(Ctx *ctx, size_t bytes);
 // Symmetric CSR in the canonical neighbour order (ig_adjacency.cu).
 ig_status build_adjacency(Ctx *ctx, Graph *g);
+// That adjacency bit-packed per row -- gap width, first neighbour, gaps
+// minus one in that width -- for the host greedy (ig_packrows.cu).
+ig_status build_packed_rows(Ctx *ctx, Graph *g);
 // Nearest-centre index of every word, device pointers, on the context stream
 // (ig_assign.cu).
 ig_status assign_centers(Ctx *ctx, const uint32_t *d_words, int64_t n, const uint32_t *d_centres, int32_t k, int len,
@@ -264,13 +277,19 @@ int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n
 // Greedy directly over neighbour lists already in m-order.
 int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int64_t base,
                               int32_t *order);
+// The same over bit-packed rows (ig_packrows.cu's format); adj_ptr gives the
+// degrees.
+int32_t greedy_from_packed(const int64_t *adj_ptr, const int64_t *pk_off, const uint32_t *pk, int32_t n, int64_t base,
+                           int32_t *order);
 
 // What the host greedy needs of a graph, downloaded once: the canonical
 // adjacency (order_threads = 1) or the upper CSR (other orders), plus the jobs.
 struct HostGraph {
     int order_threads = 1;
     const int64_t *ptr = nullptr;   // adjacency or row offsets, [n+1]
-    const int32_t *idx = nullptr;   // neighbour / column ids (global)
+    const int32_t *idx = nullptr;   // neighbour / column ids (global), or
+    const int64_t *pk_off = nullptr;  // ... the adjacency rows bit-packed
+    const uint32_t *pk = nullptr;
     std::shared_ptr<void> storage;  // owns ptr and idx (pinned block or heap)
     std::vector<JobSpec> jobs;
     std::vector<int64_t> job_edge_off;

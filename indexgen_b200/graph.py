@@ -120,6 +120,10 @@ class Context:
         check(lib().ig_ctx_alloc_stats(self.handle, ctypes.byref(k)), "ig_ctx_alloc_stats")
         return int(k.value)
 
+    def set_host_lists(self, form: int):
+        """Form of the lists sent to the host greedy: LISTS_AUTO, LISTS_PLAIN or LISTS_PACKED."""
+        check(lib().ig_ctx_set_host_lists(self.handle, int(form)), "ig_ctx_set_host_lists", self.handle)
+
     def set_host_budget(self, nbytes: int):
         """Host memory downloaded graphs may hold at once (0 = half of RAM)."""
         check(lib().ig_ctx_set_host_budget(self.handle, int(nbytes)), "ig_ctx_set_host_budget", self.handle)
@@ -300,6 +304,7 @@ LANES_FULL, LANES_NIBBLE, LANES_BYTE = 0, 1, 2
 
 
 FAULT_NONE, FAULT_DEVICE_ALLOC, FAULT_TILE_COPY = 0, 1, 2
+LISTS_AUTO, LISTS_PLAIN, LISTS_PACKED = 0, 1, 2
 
 
 def lane_form(L: int, min_ed: int) -> int:
@@ -664,7 +669,8 @@ def verify_dist(vecs, min_ed: int, ctx=None) -> bool:
 
 
 __all__ = [
-    "Context", "ConflictGraph", "IndexGenError", "Server", "FAULT_NONE", "FAULT_DEVICE_ALLOC", "FAULT_TILE_COPY", "build_conflict_graph", "build_batch", "solve_batch",
+    "Context", "ConflictGraph", "IndexGenError", "Server", "FAULT_NONE", "FAULT_DEVICE_ALLOC", "FAULT_TILE_COPY", "LISTS_AUTO", "LISTS_PLAIN",
+    "LISTS_PACKED", "build_conflict_graph", "build_batch", "solve_batch",
     "count_conflicts",
     "codebook_from_upper_csr", "codebook_from_adjacency", "solve", "pack_sequences", "apply_filters", "solve_edit_distance_cuda",
     "fill_adj_list_gpu", "solve_independent_set", "verify_dist", "default_context", "assign_centers",
