@@ -946,37 +946,79 @@ __global__ void __launch_bounds__(kNibThreads, 12) pair_kernel_nib(PairArgs a)
 }
 
 // Per row: in-place exclusive prefix of its segment counts; degree -> out[row+1].
-__global__ void row_prefix(uint32_t *__restrict__ counts, const JobDesc *__restrict__ jobs, int njobs,
-                           int64_t rows, int64_t *__restrict__ out)
+// A row's cells (one per segment from its band's first segment on, a
+// [segment][row] array) are split into kPrefixParts consecutive chunks, each
+// taken by its own thread: the threads of a warp hold 32 consecutive rows of
+// one chunk, so every access is coalesced, and four times as many loads are
+// in flight as with one thread per row (which left the kernel waiting on
+// memory with a quarter of the SM's warps).  Phase one sums each chunk, phase
+// two rewrites it with prefixes that start at the sum of the chunks before it
+// (its cells come back from L2).
+constexpr int kPrefixParts = 4;
+constexpr int kPrefixRows = 256 / kPrefixParts;
+
+__global__ void __launch_bounds__(256) row_prefix(uint32_t *__restrict__ counts, const JobDesc *__restrict__ jobs,
+                                                  int njobs, int64_t rows, int64_t *__restrict__ out)
 {
-    const int64_t gr = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (gr >= rows)
-        return;
-    const JobDesc J = jobs[find_job_by_row(jobs, njobs, gr)];
-    const int64_t row = gr - J.word_off;
-    const int g = (int)(((row / kBandRows) * kBandRows) >> J.seg_shift);
+    __shared__ uint32_t part_sum[kPrefixParts][kPrefixRows];
+    const int r = threadIdx.x % kPrefixRows, q = threadIdx.x / kPrefixRows;
+    const int64_t gr = blockIdx.x * (int64_t)kPrefixRows + r;
+    const bool live = gr < rows;
+    uint32_t *p = nullptr;
+    int64_t stride = 0;
+    int len = 0;
+    if (live) {
+        const JobDesc J = jobs[find_job_by_row(jobs, njobs, gr)];
+        const int64_t row = gr - J.word_off;
+        const int g = (int)(((row / kBandRows) * kBandRows) >> J.seg_shift);
+        const int m = max(J.nseg - g, 0);
+        const int chunk = (m + kPrefixParts - 1) / kPrefixParts;
+        const int s0 = min(q * chunk, m), s1 = min(s0 + chunk, m);
+        stride = J.n;
+        p = counts + J.count_off + (int64_t)(g + s0) * J.n + row;
+        len = s1 - s0;
+    }
+    uint32_t sum = 0;
+    {
+        int k = 0;
+        for (; k + 8 <= len; k += 8) {
+            uint32_t c[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                c[t] = p[(int64_t)(k + t) * stride];
+#pragma unroll
+            for (int t = 0; t < 8; ++t)
+                sum += c[t];
+        }
+        for (; k < len; ++k)
+            sum += p[(int64_t)k * stride];
+    }
+    part_sum[q][r] = sum;
+    __syncthreads();
     uint32_t acc = 0;
-    uint32_t *p = counts + J.count_off + (int64_t)g * J.n + row;
-    int s = g;
-    // eight cells per round, loaded before any is rewritten, so a thread keeps
-    // eight DRAM reads in flight instead of one
-    for (; s + 8 <= J.nseg; s += 8, p += 8 * (int64_t)J.n) {
-        uint32_t c[8];
+    for (int t = 0; t < q; ++t)
+        acc += part_sum[t][r];
+    {
+        int k = 0;
+        for (; k + 8 <= len; k += 8) {
+            uint32_t c[8];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-            c[k] = p[(int64_t)k * J.n];
+            for (int t = 0; t < 8; ++t)
+                c[t] = p[(int64_t)(k + t) * stride];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            p[(int64_t)k * J.n] = acc;
-            acc += c[k];
+            for (int t = 0; t < 8; ++t) {
+                p[(int64_t)(k + t) * stride] = acc;
+                acc += c[t];
+            }
+        }
+        for (; k < len; ++k) {
+            const uint32_t c = p[(int64_t)k * stride];
+            p[(int64_t)k * stride] = acc;
+            acc += c;
         }
     }
-    for (; s < J.nseg; ++s, p += J.n) {
-        const uint32_t c = *p;
-        *p = acc;
-        acc += c;
-    }
-    out[gr + 1] = (int64_t)acc;
+    if (live && q == kPrefixParts - 1)
+        out[gr + 1] = (int64_t)acc;
 }
 
 // Row offsets at job boundaries: out[j] = row_ptr[word_off_j], out[k] = row_ptr[rows].
@@ -1103,7 +1145,7 @@ __device__ __forceinline__ int find_job_by_cell(const JobDesc *jobs, int njobs, 
 // written stay in L2 while their sectors fill; each thread keeps kScatterIlp
 // records in flight.  A record whose cell or destination lies outside the
 // arrays is skipped (sentinels, and nothing else on a complete pass).
-constexpr int kScatterIlp = 4;
+constexpr int kScatterIlp = 8;
 
 __device__ __forceinline__ void scatter_one(uint2 r, const JobDesc *__restrict__ jobs, int njobs,
                                             unsigned long long ncells, const int64_t *__restrict__ row_ptr,
@@ -1521,8 +1563,8 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
             if ((e = cudaMemsetAsync(out->row_ptr, 0, sizeof(int64_t), st)) != cudaSuccess)
                 return e;
             phase_begin(ctx, IG_PHASE_COMPACT);
-            row_prefix<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(static_cast<uint32_t *>(ctx->counts.ptr),
-                                                                       d_jobs, njobs, n, out->row_ptr);
+            row_prefix<<<(unsigned)((n + kPrefixRows - 1) / kPrefixRows), 256, 0, st>>>(
+                static_cast<uint32_t *>(ctx->counts.ptr), d_jobs, njobs, n, out->row_ptr);
             launched++;
             if ((e = cudaGetLastError()) != cudaSuccess)
                 return e;
