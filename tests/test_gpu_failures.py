@@ -152,3 +152,47 @@ def test_every_allocation_of_a_batch_can_fail(oracle):
 
     failed = _alloc_sweep(run, check)
     assert len(failed) >= 6, failed
+
+
+def test_tiny_host_budget_serialises_downloads_without_deadlock(oracle):
+    """A 1 MB host budget is smaller than every graph below: each download then
+    waits until no other graph is held on the host, so batch groups, threads
+    calling solve (coalesced or not) and the server take turns -- and still
+    finish with the exact codebooks."""
+    import threading
+
+    from indexgen_b200 import Context, Server, solve, solve_batch
+
+    jobs = [(_words(6000 + 700 * j, L, 300 + j), L, d) for j, (L, d) in enumerate([(11, 3), (10, 4), (12, 4), (10, 5)])]
+    want = []
+    for w, L, d in jobs:
+        rp, cols = oracle.conflict_upper(w, L, d)
+        want.append(oracle.codebook(rp, cols, len(w), 1))
+    ctx = Context(0)
+    try:
+        ctx.set_host_budget(1 << 20)
+        assert ctx.host_budget()[0] == 1 << 20
+        books, _ = solve_batch(jobs, 1, 0, ctx)
+        for got, exp in zip(books, want):
+            assert np.array_equal(got, exp)
+        for coalesce in (True, False):
+            ctx.set_coalescing(coalesce)
+            got = [None] * len(jobs)
+
+            def run(i):
+                got[i] = solve(*jobs[i], 1, ctx)[0]
+
+            ts = [threading.Thread(target=run, args=(i,)) for i in range(len(jobs)) for _ in range(2)]
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+            for g, exp in zip(got, want):
+                assert np.array_equal(g, exp)
+        with Server(ctx, host_threads=3) as sv:
+            tickets = [sv.submit(*j) for j in jobs]
+            for t, exp in zip(tickets, want):
+                assert np.array_equal(sv.wait(t)[0], exp)
+        assert ctx.host_budget()[1] == 0  # every download's share came back
+    finally:
+        ctx.close()
