@@ -362,6 +362,19 @@ ig_status ig_codebook_from_adjacency(const int64_t *adj_ptr, const int32_t *adj,
 /* Greedy over a caller-supplied upper CSR in host memory (no device work). */
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count);
+/* No counterpart in the reference (its greedy is single-threaded).  Every
+ * greedy of this library (ig_solve, batches, the server, the two calls above)
+ * over a graph with at least min_entries neighbour-list entries (twice its
+ * edges) runs on two threads -- the caller walks the balls and keeps the
+ * degrees, a helper thread keeps the degree buckets -- while fewer than
+ * max_helpers such helper threads are running in the process; otherwise it
+ * runs on the calling thread alone.  Both forms give the same codebook.
+ * Process-wide.  max_helpers < 0: (hardware threads - 1) / 2; 0: never.
+ * min_entries < 0: 2^20. */
+ig_status ig_set_greedy_threads(int max_helpers, int64_t min_entries);
+/* Greedies run so far in this process, two-threaded and single-threaded
+ * (either pointer may be null). */
+ig_status ig_greedy_stats(int64_t *pipelined, int64_t *sequential);
 
 /* ---- allocation-free variant ------------------------------------------- */
 

@@ -31,10 +31,12 @@ from .graph import (  # noqa: F401
     count_conflicts,
     default_context,
     fill_adj_list_gpu,
+    greedy_stats,
     lane_form,
     pack_sequences,
     random_cluster_fit,
     read_adj_list,
+    set_greedy_threads,
     solve,
     solve_batch,
     solve_assignments_cuda,

@@ -20,6 +20,7 @@ EXPORTS = (
     "ig_graph_stats", "ig_graph_upper_csr", "ig_graph_pairs", "ig_graph_device_csr", "ig_graph_adjacency",
     "ig_graph_device_adjacency", "ig_graph_codebook",
     "ig_solve", "ig_count_conflicts", "ig_codebook_from_adjacency", "ig_codebook_from_upper_csr", "ig_count_conflicts_noalloc",
+    "ig_set_greedy_threads", "ig_greedy_stats",
     "ig_assign_centers", "ig_cluster_solve", "ig_graph_write_adj_list", "ig_graph_read_adj_list",
     "ig_batch_build", "ig_graph_job_count", "ig_graph_job_stats", "ig_graph_job_tiling", "ig_graph_job_codebooks", "ig_solve_batch",
     "ig_server_create", "ig_server_submit", "ig_server_poll", "ig_server_wait", "ig_server_cancel",
@@ -84,6 +85,8 @@ def _declare(L):
         "ig_count_conflicts": (_int, [_vp, _vp, _i32, _int, _int, ctypes.POINTER(_i64)]),
         "ig_codebook_from_upper_csr": (_int, [_vp, _vp, _i32, _int, _vp, ctypes.POINTER(_i32)]),
         "ig_codebook_from_adjacency": (_int, [_vp, _vp, _i32, _vp, ctypes.POINTER(_i32)]),
+        "ig_set_greedy_threads": (_int, [_int, _i64]),
+        "ig_greedy_stats": (_int, [ctypes.POINTER(_i64), ctypes.POINTER(_i64)]),
         "ig_count_conflicts_noalloc": (_int, [_vp, _i32, _int, _int, _vp, _vp]),
         "ig_assign_centers": (_int, [_vp, _vp, _i64, _vp, _i32, _int, _int, _vp]),
         "ig_graph_write_adj_list": (_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_i64)]),

@@ -1,20 +1,77 @@
 // Host-side parts of libindexgen_cuda: input packing, candidate filters and
-// the sequential greedy independent set.
+// the greedy independent set.
 //
 // The greedy is a sequential bucket-queue walk whose every step depends on the
 // previous one (a chain of dependent loads and stores per removed edge); it is
 // latency-bound pointer chasing, so it runs on the host next to the device CSR
-// it consumes, as the reference's AdjList does.
+// it consumes, as the reference's AdjList does.  Large graphs split each step
+// over two threads (PipelinedGreedy): one walks the balls and keeps the
+// degrees, the other keeps the degree buckets.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
+#include <system_error>
+#include <thread>
 #include <vector>
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 #include "ig_internal.h"
 
 namespace ig {
 
 namespace {
+
+// Helper threads of pipelined greedies in use in this process, and the limits
+// set by ig_set_greedy_threads (negative = default).
+std::atomic<int> g_helpers_busy{0};
+std::atomic<int> g_helpers_max{-1};
+std::atomic<int64_t> g_pipeline_min{-1};
+std::atomic<int64_t> g_runs_pipelined{0};
+std::atomic<int64_t> g_runs_sequential{0};
+constexpr int64_t kPipelineMinEntries = int64_t(1) << 20;
+
+inline void cpu_relax()
+{
+#if defined(__x86_64__)
+    _mm_pause();
+#endif
+}
+
+// The two threads of a pipelined greedy wait on each other once per ball:
+// spin briefly, then yield so that an oversubscribed host still runs the
+// other thread.
+struct Backoff {
+    int spins = 0;
+    void pause()
+    {
+        if (++spins < 4096)
+            cpu_relax();
+        else
+            std::this_thread::yield();
+    }
+};
+
+int helper_cap()
+{
+    const int m = g_helpers_max.load();
+    if (m >= 0)
+        return m;
+    const int hc = (int)std::thread::hardware_concurrency();
+    return std::max(0, (hc - 1) / 2);
+}
+
+bool take_helper()
+{
+    const int cap = helper_cap();
+    int cur = g_helpers_busy.load();
+    while (cur < cap)
+        if (g_helpers_busy.compare_exchange_weak(cur, cur + 1))
+            return true;
+    return false;
+}
 
 // Neighbour lists in the order FillAdjList(T) assembles them
 // (src/SparseMat.cpp:599-609): thread t holds pairs (i, j) with i = t (mod T),
@@ -289,6 +346,238 @@ class BucketGreedy {
     int32_t active_ = 0;
 };
 
+// BucketGreedy's walk split over two threads, with the same result.
+//
+// With the live-neighbour test made branch-free, the sequential walk spends
+// its time in two halves of similar cost: loading and lowering the degrees of
+// the neighbours, and moving those neighbours between degree buckets.  Here
+// the calling thread (the walker) selects the vertices, collects each ball and
+// keeps the degrees: for every neighbour it loads the degree, lowers it if
+// positive, and writes the bucket move (vertex, old degree) into a ring whose
+// cursor advances only for live neighbours, followed by the deletion
+// (vertex, final degree) of each ball vertex.  A helper thread (the mover)
+// applies the ring in order to the buckets with BucketGreedy's own
+// delete_row / decrease_sum steps and keeps the minimum tracker.  Every
+// bucket therefore sees exactly the sequential sequence of appends and
+// swap-removals.  Before each selection the walker waits until the mover has
+// applied everything written, then reads the back of the minimum bucket.
+//
+// Degrees (walker) and bucket positions (mover) live in separate arrays so
+// neither thread writes a cache line the other one is using.
+template <class Rows>
+class PipelinedGreedy {
+  public:
+    PipelinedGreedy(const int64_t *ap, Rows rows, int32_t n, int64_t base)
+        : ap_(ap), rows_(rows), base_(base), n_(n), deg_((size_t)n), pos_((size_t)n)
+    {
+        int32_t maxd = 0;
+        for (int32_t i = 0; i < n; ++i) {
+            deg_[(size_t)i] = (int32_t)(ap[i + 1] - ap[i]);
+            maxd = std::max(maxd, deg_[(size_t)i]);
+        }
+        nb_ = maxd + 1;
+        std::vector<int64_t> hist((size_t)nb_ + 1, 0);
+        for (int32_t i = 0; i < n; ++i)
+            hist[(size_t)deg_[(size_t)i]]++;
+        start_.resize((size_t)nb_ + 1);
+        size_.assign((size_t)nb_, 0);
+        int64_t ge = n, off = 0;
+        for (int32_t b = 0; b < nb_; ++b) {
+            start_[(size_t)b] = off;
+            off += ge;
+            ge -= hist[(size_t)b];
+        }
+        start_[(size_t)nb_] = off;
+        data_.reset(new int32_t[(size_t)std::max<int64_t>(off, 1)]);
+        int32_t tracker = maxd + 1;
+        for (int32_t i = 0; i < n; ++i) {
+            const int32_t d = deg_[(size_t)i];
+            pos_[(size_t)i] = size_[(size_t)d];
+            data_[(size_t)(start_[(size_t)d] + size_[(size_t)d]++)] = i;
+            tracker = std::min(tracker, d);
+        }
+        tracker_.store(tracker);
+        todel_.resize((size_t)maxd + 1);
+        bufx_.resize((size_t)maxd + 1);
+        bufi_.resize((size_t)maxd + 1);
+        ring_.reset(new uint64_t[(size_t)kRing]);
+    }
+
+    // The selection's size, or -1 when the mover thread could not be started
+    // (nothing has been changed then; the caller runs BucketGreedy).
+    int32_t run(int32_t *order)
+    {
+        std::thread mover;
+        try {
+            mover = std::thread([this]() { move_loop(); });
+        } catch (const std::system_error &) {
+            return -1;
+        }
+        int32_t *deg = deg_.data();
+        uint64_t *ring = ring_.get();
+        int64_t p = 0;  // ring entries written
+        int32_t cnt = 0, active = n_;
+        while (active > 0) {
+            // MinSumRow once every move so far is in the buckets
+            pub_.store(p, std::memory_order_release);
+            for (Backoff bo; cons_.load(std::memory_order_acquire) < p;)
+                bo.pause();
+            const int32_t t = tracker_.load(std::memory_order_relaxed);
+            const int32_t x = data_[(size_t)(start_[(size_t)t] + size_[(size_t)t] - 1)];
+            order[cnt++] = x;
+            // DelBall: active neighbours in m-order, then the vertex itself
+            const int32_t *row = rows_.get(x, bufx_.data());
+            const int64_t len = ap_[x + 1] - ap_[x];
+            int32_t nt = 0;
+            for (int64_t k = 0; k < len; ++k) {
+                const int32_t j = (int32_t)(row[k] - base_);
+                todel_[(size_t)nt] = j;
+                nt += deg[j] >= 0;
+            }
+            todel_[(size_t)nt++] = x;
+            for (int32_t q = 0; q < nt && q < 4; ++q)
+                rows_.prefetch(todel_[(size_t)q]);
+            for (int32_t q = 0; q < nt; ++q) {
+                if (q + 4 < nt)
+                    rows_.prefetch(todel_[(size_t)q + 4]);
+                const int32_t i = todel_[(size_t)q];
+                if (deg[i] < 0)
+                    continue;
+                const int32_t *ri = rows_.get(i, bufi_.data());
+                const int64_t e = ap_[i + 1] - ap_[i];
+                // chunks of at most kChunk neighbours; room for the chunk and
+                // the deletion that may follow it is waited for first
+                for (int64_t k0 = 0;; k0 += kChunk) {
+                    const int64_t k1 = std::min<int64_t>(e, k0 + kChunk);
+                    pub_.store(p, std::memory_order_release);
+                    for (Backoff bo; p + kChunk + 1 - cons_.load(std::memory_order_acquire) > kRing;)
+                        bo.pause();
+                    for (int64_t k = k0; k < k1; ++k) {
+                        if (k + 16 < e)
+                            __builtin_prefetch(deg + (ri[k + 16] - base_));
+                        const int32_t j = (int32_t)(ri[k] - base_);
+                        const int32_t d = deg[j];
+                        ring[p & (kRing - 1)] = ((uint64_t)(uint32_t)d << 32) | (uint32_t)j;
+                        deg[j] = d - (d > 0);
+                        p += d > 0;
+                    }
+                    if (k1 >= e)
+                        break;
+                }
+                ring[p & (kRing - 1)] = ((uint64_t)(uint32_t)deg[i] << 32) | (uint32_t)i | kDelete;
+                ++p;
+                deg[i] = -1;
+                --active;
+            }
+        }
+        pub_.store(p, std::memory_order_release);
+        done_.store(true, std::memory_order_release);
+        mover.join();
+        return cnt;
+    }
+
+  private:
+    static constexpr int64_t kRing = int64_t(1) << 16;  // entries (512 KB)
+    static constexpr int64_t kChunk = 4096;
+    static constexpr uint64_t kDelete = uint64_t(1) << 31;
+
+    void move_loop()
+    {
+        int32_t *pos = pos_.data();
+        int32_t *sz = size_.data();
+        const int64_t *start = start_.data();
+        int32_t *data = data_.get();
+        const uint64_t *ring = ring_.get();
+        int32_t tracker = tracker_.load(std::memory_order_relaxed);
+        int64_t c = 0;
+        for (Backoff bo;;) {
+            const int64_t p = pub_.load(std::memory_order_acquire);
+            if (c == p) {
+                if (done_.load(std::memory_order_acquire) && pub_.load(std::memory_order_acquire) == c)
+                    return;
+                bo.pause();
+                continue;
+            }
+            bo.spins = 0;
+            for (; c < p; ++c) {
+                if (c + 16 < p)
+                    __builtin_prefetch(pos + ((uint32_t)ring[(c + 16) & (kRing - 1)] & 0x7fffffffu));
+                const uint64_t op = ring[c & (kRing - 1)];
+                const int32_t v = (int32_t)((uint32_t)op & 0x7fffffffu);
+                const int32_t cur = (int32_t)(op >> 32);
+                // delete_row(cur, v)
+                const int64_t base = start[cur];
+                const int32_t s = --sz[cur];
+                const int32_t q = pos[v];
+                const int32_t last = data[base + s];
+                data[base + q] = last;
+                pos[last] = q;
+                if (cur == tracker && s == 0)
+                    while (tracker < nb_ && sz[tracker] == 0)
+                        ++tracker;
+                if (!(op & kDelete)) {  // decrease_sum: append to the bucket below
+                    const int32_t b = cur - 1;
+                    const int32_t s1 = sz[b]++;
+                    data[start[b] + s1] = v;
+                    pos[v] = s1;
+                    if (b < tracker)
+                        tracker = b;
+                }
+                if ((c & 1023) == 1023) {
+                    tracker_.store(tracker, std::memory_order_relaxed);
+                    cons_.store(c + 1, std::memory_order_release);
+                }
+            }
+            tracker_.store(tracker, std::memory_order_relaxed);
+            cons_.store(c, std::memory_order_release);
+        }
+    }
+
+    const int64_t *ap_;
+    Rows rows_;
+    int64_t base_;
+    int32_t n_;
+    std::vector<int32_t> deg_;  // walker: current degree, -1 once deleted
+    std::vector<int32_t> pos_;  // mover: slot inside the degree bucket
+    std::vector<int32_t> size_;
+    std::vector<int64_t> start_;
+    std::unique_ptr<int32_t[]> data_;
+    std::unique_ptr<uint64_t[]> ring_;
+    std::vector<int32_t> todel_, bufx_, bufi_;
+    int32_t nb_ = 0;
+    alignas(64) std::atomic<int64_t> pub_{0};   // entries the walker has published
+    alignas(64) std::atomic<int64_t> cons_{0};  // entries the mover has applied
+    alignas(64) std::atomic<int32_t> tracker_{0};
+    alignas(64) std::atomic<bool> done_{false};
+};
+
+// A greedy over n rows: pipelined over two threads when the graph has at
+// least the configured number of neighbour-list entries and a helper thread
+// is free in this process, else sequential on the calling thread.
+template <class Rows>
+int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_t *order)
+{
+    if (n <= 0)
+        return 0;
+    int64_t min_entries = g_pipeline_min.load();
+    if (min_entries < 0)
+        min_entries = kPipelineMinEntries;
+    if (ap[n] - ap[0] >= min_entries && take_helper()) {
+        struct Give {
+            ~Give() { g_helpers_busy.fetch_sub(1); }
+        } give;
+        PipelinedGreedy<Rows> g(ap, rows, n, base);
+        const int32_t cnt = g.run(order);
+        if (cnt >= 0) {
+            g_runs_pipelined++;
+            return cnt;
+        }
+    }
+    g_runs_sequential++;
+    BucketGreedy<Rows> g(ap, rows, n, base);
+    return g.run(order);
+}
+
 }  // namespace
 
 int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int64_t base, int order_threads,
@@ -299,25 +588,18 @@ int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n
     std::vector<int64_t> ap;
     std::vector<int32_t> adj;
     assemble(row_ptr, cols, n, base, order_threads, ap, adj);
-    BucketGreedy<PlainRows> g(ap.data(), PlainRows{ap.data(), adj.data()}, n, 0);
-    return g.run(order);
+    return run_greedy(ap.data(), PlainRows{ap.data(), adj.data()}, n, 0, order);
 }
 
 int32_t greedy_from_adjacency(const int64_t *adj_ptr, const int32_t *adj, int32_t n, int64_t base, int32_t *order)
 {
-    if (n <= 0)
-        return 0;
-    BucketGreedy<PlainRows> g(adj_ptr, PlainRows{adj_ptr, adj}, n, base);
-    return g.run(order);
+    return run_greedy(adj_ptr, PlainRows{adj_ptr, adj}, n, base, order);
 }
 
 int32_t greedy_from_packed(const int64_t *adj_ptr, const int64_t *pk_off, const uint32_t *pk, int32_t n, int64_t base,
                            int32_t *order)
 {
-    if (n <= 0)
-        return 0;
-    BucketGreedy<PackedRows> g(adj_ptr, PackedRows{adj_ptr, pk_off, pk}, n, base);
-    return g.run(order);
+    return run_greedy(adj_ptr, PackedRows{adj_ptr, pk_off, pk}, n, base, order);
 }
 
 }  // namespace ig
@@ -406,6 +688,26 @@ ig_status ig_codebook_from_adjacency(const int64_t *adj_ptr, const int32_t *adj,
     } catch (...) {
         return IG_ERR_OOM;
     }
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_set_greedy_threads(int max_helpers, int64_t min_entries)
+{
+    IG_ABI_TRY
+    ig::g_helpers_max.store(max_helpers < 0 ? -1 : max_helpers);
+    ig::g_pipeline_min.store(min_entries < 0 ? -1 : min_entries);
+    return IG_OK;
+    IG_ABI_CATCH
+}
+
+ig_status ig_greedy_stats(int64_t *pipelined, int64_t *sequential)
+{
+    IG_ABI_TRY
+    if (pipelined)
+        *pipelined = ig::g_runs_pipelined.load();
+    if (sequential)
+        *sequential = ig::g_runs_sequential.load();
     return IG_OK;
     IG_ABI_CATCH
 }

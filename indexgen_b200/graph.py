@@ -421,6 +421,22 @@ def codebook_from_adjacency(adj_ptr, adj, n: int) -> np.ndarray:
     return order[: cnt.value].copy()
 
 
+def set_greedy_threads(max_helpers: int = -1, min_entries: int = -1) -> None:
+    """Process-wide threading of the host greedy: a greedy over a graph with at
+    least `min_entries` neighbour-list entries runs on two threads while fewer
+    than `max_helpers` helper threads are in use (defaults: 2^20 entries,
+    (hardware threads - 1) // 2 helpers; 0 helpers = always one thread).  The
+    codebook is the same either way."""
+    check(lib().ig_set_greedy_threads(int(max_helpers), int(min_entries)), "ig_set_greedy_threads")
+
+
+def greedy_stats() -> tuple:
+    """(two-threaded, single-threaded) greedies run so far in this process."""
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    check(lib().ig_greedy_stats(ctypes.byref(a), ctypes.byref(b)), "ig_greedy_stats")
+    return a.value, b.value
+
+
 def codebook_from_upper_csr(row_ptr, cols, n: int, order_threads: int = 1) -> np.ndarray:
     rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
     cl = np.ascontiguousarray(cols, dtype=np.int32)

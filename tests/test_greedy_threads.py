@@ -1,0 +1,136 @@
+"""The two-threaded host greedy (one thread walks the balls and keeps the
+degrees, a helper thread keeps the degree buckets) against the single-threaded
+one and the oracle's restatement of the reference's AdjList greedy: the same
+codebook sequence on every graph, including rows longer than the walker's
+chunk, more bucket moves than the ring holds, cliques, stars, isolated
+vertices, both neighbour-list orders, and several greedies running at once
+with fewer helper threads than greedies.  Host-only (no device work).
+Integer work: bit-exact."""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+
+
+@pytest.fixture(scope="module")
+def G():
+    from indexgen_b200 import build as B
+
+    B.build()
+    import indexgen_b200 as G
+
+    yield G
+    G.set_greedy_threads(-1, -1)
+
+
+def upper_csr(n, pairs):
+    """Upper CSR of the undirected edge set `pairs` (any orientation, repeats dropped)."""
+    p = np.asarray(pairs, dtype=np.int64).reshape(-1, 2)
+    p = p[p[:, 0] != p[:, 1]]
+    p = np.sort(p, axis=1)
+    p = np.unique(p, axis=0)
+    row_ptr = np.zeros(n + 1, np.int64)
+    np.add.at(row_ptr, p[:, 0] + 1, 1)
+    return np.cumsum(row_ptr), p[:, 1].astype(np.int32)
+
+
+def graphs():
+    rng = np.random.default_rng(11)
+    out = {}
+    n = 5000
+    out["sparse"] = (n, upper_csr(n, rng.integers(0, n, (60000, 2))))
+    n = 40000  # ~4e5 bucket moves: the ring (65536 entries) wraps several times
+    out["wrap"] = (n, upper_csr(n, rng.integers(0, n, (400000, 2))))
+    n = 12001  # a hub of degree 12000: rows longer than one walker chunk (4096)
+    star = np.stack([np.zeros(n - 1, np.int64), np.arange(1, n)], axis=1)
+    out["star"] = (n, upper_csr(n, np.concatenate([star, rng.integers(1, n, (30000, 2))])))
+    n = 300  # every degree equal
+    iu = np.triu_indices(n, 1)
+    out["clique"] = (n, upper_csr(n, np.stack(iu, axis=1)))
+    n = 3000  # isolated vertices, pairs and a dense core
+    core = rng.integers(0, 400, (20000, 2))
+    pairs = np.stack([np.arange(1000, 2000, 2), np.arange(1001, 2001, 2)], axis=1)
+    out["mixed"] = (n, upper_csr(n, np.concatenate([core, pairs])))
+    return out
+
+
+def both(G, fn):
+    G.set_greedy_threads(0, -1)
+    seq = fn()
+    G.set_greedy_threads(1, 0)
+    before = G.greedy_stats()[0]
+    par = fn()
+    assert G.greedy_stats()[0] > before, "the two-threaded greedy did not run"
+    G.set_greedy_threads(-1, -1)
+    return seq, par
+
+
+@pytest.mark.parametrize("name", ["sparse", "wrap", "star", "clique", "mixed"])
+def test_two_threads_equal_one_and_oracle(G, oracle, name):
+    n, (rp, cols) = graphs()[name]
+    want = oracle.codebook(rp, cols, n, 1)
+    seq, par = both(G, lambda: G.codebook_from_upper_csr(rp, cols, n, 1))
+    assert np.array_equal(seq, want)
+    assert np.array_equal(par, want)
+    # the FillAdjList(T) neighbour order changes the codebook; both forms follow it
+    want3 = oracle.codebook(rp, cols, n, 3)
+    ap, adj = oracle.adjacency(rp, cols, n, 3)
+    seq, par = both(G, lambda: G.codebook_from_adjacency(ap, adj, n))
+    assert np.array_equal(seq, want3)
+    assert np.array_equal(par, want3)
+
+
+def test_two_threads_reference_fixtures(G):
+    g = load_golden("uniform11.npz")
+    n = len(g["words"])
+    e = g["edges"]
+    rp = np.zeros(n + 1, np.int64)
+    np.add.at(rp, e[:, 0].astype(np.int64) + 1, 1)
+    rp = np.cumsum(rp)
+    for T in (1, 8, 16):
+        seq, par = both(G, lambda: G.codebook_from_upper_csr(rp, e[:, 1], n, T))
+        assert np.array_equal(seq, g[f"sel{T}"])
+        assert np.array_equal(par, g[f"sel{T}"])
+    s = load_golden("small_cases.npz")
+    for key in sorted({k[: -len("_adj3_ptr")] for k in s.files if k.endswith("_adj3_ptr")}):
+        m = len(s[key + "_adj3_ptr"]) - 1
+        seq, par = both(G, lambda: G.codebook_from_adjacency(s[key + "_adj3_ptr"], s[key + "_adj3"], m))
+        assert np.array_equal(seq, par), key
+        assert np.array_equal(par, s[key + "_sel3"]), key
+
+
+def test_concurrent_greedies_share_a_helper(G, oracle):
+    """Six greedies at once with one helper thread allowed: some run
+    two-threaded, the rest single-threaded; every result is the oracle's."""
+    n, (rp, cols) = graphs()["wrap"]
+    want = oracle.codebook(rp, cols, n, 1)
+    G.set_greedy_threads(1, 0)
+    p0, s0 = G.greedy_stats()
+    results = [None] * 6
+
+    def run(k):
+        results[k] = G.codebook_from_upper_csr(rp, cols, n, 1)
+
+    ts = [threading.Thread(target=run, args=(k,)) for k in range(6)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    p1, s1 = G.greedy_stats()
+    G.set_greedy_threads(-1, -1)
+    assert (p1 - p0) + (s1 - s0) == 6
+    assert p1 - p0 >= 1
+    for r in results:
+        assert np.array_equal(r, want)
+
+
+def test_small_graphs_stay_single_threaded(G):
+    G.set_greedy_threads(-1, -1)
+    p0, s0 = G.greedy_stats()
+    rp = np.array([0, 1, 2, 2], np.int64)
+    cols = np.array([1, 2], np.int32)
+    assert G.codebook_from_upper_csr(rp, cols, 3, 1).tolist() == [2, 0]
+    p1, s1 = G.greedy_stats()
+    assert (p1, s1) == (p0, s0 + 1)
