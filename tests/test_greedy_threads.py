@@ -134,3 +134,32 @@ def test_small_graphs_stay_single_threaded(G):
     assert G.codebook_from_upper_csr(rp, cols, 3, 1).tolist() == [2, 0]
     p1, s1 = G.greedy_stats()
     assert (p1, s1) == (p0, s0 + 1)
+
+
+@pytest.mark.gpu
+def test_two_threads_on_the_linear12_job(igctx):
+    """words -> codebook for the [12,9,3] GF(4) code + coset job (207,432
+    words, editDist 4) through ig_solve, with the greedy on two threads (the
+    default at this size) and on one: both equal the reference's codebook."""
+    import hashlib
+    import json
+    import os
+
+    from conftest import GOLDEN
+    from indexgen_b200 import greedy_stats, set_greedy_threads, solve
+    from indexgen_b200 import workloads as W
+
+    gold = json.load(open(os.path.join(GOLDEN, "linear.json")))["linear12"]
+    words = W.linear12_candidates()
+    try:
+        set_greedy_threads(1, -1)
+        p0 = greedy_stats()[0]
+        two, edges = solve(words, 12, 4, 1, igctx)
+        assert greedy_stats()[0] == p0 + 1
+        set_greedy_threads(0, -1)
+        one, _ = solve(words, 12, 4, 1, igctx)
+    finally:
+        set_greedy_threads(-1, -1)
+    assert edges == gold["edges"]
+    assert np.array_equal(two, one)
+    assert hashlib.sha256(two.astype("<i4").tobytes()).hexdigest() == gold["codebook_t1_sha256"]
