@@ -266,6 +266,16 @@ def profile_traffic(wl_name):
     return None
 
 
+def touched_cells(n: int, seg_width: int, segments: int, band_rows: int = 256) -> int:
+    """(row, segment) count cells the pair kernel writes and the compaction
+    reads: a row's cells run from its band's first segment on (band_rows-row
+    bands, segments of seg_width columns, upper triangle only)."""
+    bands = np.arange((n + band_rows - 1) // band_rows, dtype=np.int64)
+    rows = np.minimum(band_rows, n - bands * band_rows)
+    first = (bands * band_rows) // seg_width
+    return int(np.sum(rows * np.maximum(segments - first, 0)))
+
+
 def alu_ops_per_pair(L: int, d: int) -> float:
     """ALU-pipe operations (LOP3, PRMT, the add and the shift) the pair-test
     recurrence issues per pair test, counted from the kernel source (the lane
@@ -784,6 +794,8 @@ def run_ours(args, wl, rank, world, dist):
     total_ms = sum(step_ms)
     pair_ms, pair_launches = ctx.phase_time(0)
     comp_ms, comp_launches = ctx.phase_time(1)
+    comp_parts = {name: ctx.phase_time(ph)[0] / max(ctx.phase_time(ph)[1], 1)
+                  for name, ph in (("prefix_ms", 3), ("scan_ms", 4), ("scatter_ms", 5))}
     ctx.set_profiling(False)
     total_ms = max_over_ranks(total_ms, dist, f"cuda:{dev}")
     value = replica_rate(world, pairs, args.steps, total_ms / 1e3)
@@ -886,9 +898,10 @@ def run_ours(args, wl, rank, world, dist):
     traffic = profile_traffic(wl["name"])
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     # compaction: 8 B edge record read + 4 B column written per edge, 4 B
-    # count read + 4 B prefix written per (row, segment) cell, 24 B per row
-    # (degree, offset scan, offset read)
-    cells = segments * n
+    # count read + 4 B prefix written per (row, segment) cell a row uses (its
+    # band's diagonal segment onwards), 24 B per row (degree, offset scan,
+    # offset read)
+    cells = touched_cells(n, seg_width, segments)
     comp_bytes = 12 * edges + 8 * cells + 24 * (n + 1)
     comp_avg_s = (comp_ms / max(comp_launches, 1)) / 1e3
     line = {
@@ -915,7 +928,8 @@ def run_ours(args, wl, rank, world, dist):
                        "peak": hbm_peak, "unit": "GB/s",
                        "frac": (comp_bytes / comp_avg_s / 1e9 / hbm_peak) if comp_launches else None,
                        "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs",
-                       "bytes_per_launch": comp_bytes, "count_cells": cells, "segment_width": seg_width},
+                       "bytes_per_launch": comp_bytes, "count_cells": cells, "segment_width": seg_width,
+                       "parts_ms_per_launch": comp_parts},
         "gpu_launches": launches,
         "work_split": {"lane_form": ["full", "nibble", "byte"][lane_form(L, d)],
                        "items_per_cta": ctx.work_split(lane_form(L, d))[0],

@@ -62,12 +62,17 @@ ig_status ig_ctx_reserve(ig_ctx *ctx, int64_t edges);
 int64_t ig_ctx_launches(const ig_ctx *ctx);
 /* Per-phase device timing with CUDA events on the context's stream (off by
  * default).  Phases: IG_PHASE_PAIRS (the pair-test kernel), IG_PHASE_COMPACT
- * (row prefix + scan + scatter into CSR), IG_PHASE_PREP (selector streams).
- * ig_ctx_phase_time returns the accumulated milliseconds and launch count
- * since profiling was last enabled. */
+ * (row prefix + scan + scatter into CSR), IG_PHASE_PREP (selector streams),
+ * and the three parts of IG_PHASE_COMPACT: IG_PHASE_PREFIX (per-row prefix
+ * of the segment counts), IG_PHASE_SCAN (row offsets), IG_PHASE_SCATTER
+ * (records into columns).  ig_ctx_phase_time returns the accumulated
+ * milliseconds and launch count since profiling was last enabled. */
 #define IG_PHASE_PAIRS 0
 #define IG_PHASE_COMPACT 1
 #define IG_PHASE_PREP 2
+#define IG_PHASE_PREFIX 3
+#define IG_PHASE_SCAN 4
+#define IG_PHASE_SCATTER 5
 ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable);
 ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches);
 

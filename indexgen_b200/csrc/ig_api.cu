@@ -1010,7 +1010,7 @@ ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable)
                 return ig::cuda_error(ctx, cudaGetLastError(), "cudaEventCreate");
     }
     ctx->profiling = enable != 0;
-    for (int p = 0; p < 3; ++p) {
+    for (int p = 0; p < ig::Ctx::kPhases; ++p) {
         ctx->phase_ms[p] = 0;
         ctx->phase_launches[p] = 0;
         ctx->phase_pending[p] = false;
@@ -1022,7 +1022,7 @@ ig_status ig_ctx_set_profiling(ig_ctx *ctx, int enable)
 ig_status ig_ctx_phase_time(const ig_ctx *ctx, int phase, double *ms, int64_t *launches)
 {
     IG_ABI_TRY
-    if (!ctx || phase < 0 || phase > 2)
+    if (!ctx || phase < 0 || phase >= ig::Ctx::kPhases)
         return IG_ERR_INPUT;
     if (ms)
         *ms = ctx->phase_ms[phase];

@@ -1563,14 +1563,19 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
             if ((e = cudaMemsetAsync(out->row_ptr, 0, sizeof(int64_t), st)) != cudaSuccess)
                 return e;
             phase_begin(ctx, IG_PHASE_COMPACT);
+            phase_begin(ctx, IG_PHASE_PREFIX);
             row_prefix<<<(unsigned)((n + kPrefixRows - 1) / kPrefixRows), 256, 0, st>>>(
                 static_cast<uint32_t *>(ctx->counts.ptr), d_jobs, njobs, n, out->row_ptr);
             launched++;
             if ((e = cudaGetLastError()) != cudaSuccess)
                 return e;
+            phase_end(ctx, IG_PHASE_PREFIX);
             // inclusive scan over row_ptr[0..n] (row_ptr[0] = 0) gives the offsets
+            phase_begin(ctx, IG_PHASE_SCAN);
             if (inclusive_scan_i64(ctx, out->row_ptr, m) != IG_OK)
                 return cudaErrorLaunchFailure;
+            phase_end(ctx, IG_PHASE_SCAN);
+            phase_begin(ctx, IG_PHASE_SCATTER);
             scatter_records<<<sgrid, 256, 0, st>>>(static_cast<const EdgeRecord *>(ctx->records.ptr), flags + 1,
                                                     a.status, cap, d_jobs, njobs, (unsigned long long)B.counts,
                                                     out->row_ptr, static_cast<const uint32_t *>(ctx->counts.ptr),
@@ -1578,6 +1583,7 @@ ig_status run_pass(Ctx *ctx, const uint32_t *d_words, const BatchLayout &B, int 
             launched++;
             if ((e = cudaGetLastError()) != cudaSuccess)
                 return e;
+            phase_end(ctx, IG_PHASE_SCATTER);
             phase_end(ctx, IG_PHASE_COMPACT);
             job_bounds<<<(unsigned)((njobs + 1 + 255) / 256), 256, 0, st>>>(out->row_ptr, d_jobs, njobs, n,
                                                                              d_bounds);
@@ -1680,7 +1686,7 @@ void phase_collect(Ctx *ctx)
 {
     if (!ctx->profiling)
         return;
-    for (int p = 0; p < 3; ++p) {
+    for (int p = 0; p < Ctx::kPhases; ++p) {
         if (!ctx->phase_pending[p])
             continue;
         float ms = 0.f;

@@ -145,10 +145,11 @@ struct Ctx {
     int64_t tune_runs = 0; // tuner runs that chose among several plans
     // optional per-phase timing (IG_PHASE_*)
     bool profiling = false;
-    cudaEvent_t ev[6] = {};
-    double phase_ms[3] = {0, 0, 0};
-    int64_t phase_launches[3] = {0, 0, 0};
-    bool phase_pending[3] = {false, false, false};
+    static constexpr int kPhases = 6;
+    cudaEvent_t ev[2 * kPhases] = {};
+    double phase_ms[kPhases] = {};
+    int64_t phase_launches[kPhases] = {};
+    bool phase_pending[kPhases] = {};
     std::shared_ptr<PinnedPool> pinned = std::make_shared<PinnedPool>();
     // CUDA graphs of the batch pipeline: [0] a build pass (job table upload,
     // selector streams, pair kernels, row offsets, scan, scatter into CSR,
