@@ -372,8 +372,10 @@ ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols
  * over a graph with at least min_entries neighbour-list entries (twice its
  * edges) runs on two threads -- the caller walks the balls and keeps the
  * degrees, a helper thread keeps the degree buckets -- while fewer than
- * max_helpers such helper threads are running in the process; otherwise it
- * runs on the calling thread alone.  Both forms give the same codebook.
+ * max_helpers such helper threads are running in the process and the
+ * greedies running plus the helpers stay below the hardware threads;
+ * otherwise it runs on the calling thread alone.  Both forms give the same
+ * codebook.
  * Process-wide.  max_helpers < 0: (hardware threads - 1) / 2; 0: never.
  * min_entries < 0: 2^20. */
 ig_status ig_set_greedy_threads(int max_helpers, int64_t min_entries);

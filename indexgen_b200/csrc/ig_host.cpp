@@ -24,8 +24,9 @@ namespace ig {
 
 namespace {
 
-// Helper threads of pipelined greedies in use in this process, and the limits
-// set by ig_set_greedy_threads (negative = default).
+// Greedies running and helper threads of pipelined greedies in use in this
+// process, and the limits set by ig_set_greedy_threads (negative = default).
+std::atomic<int> g_greedies_running{0};
 std::atomic<int> g_helpers_busy{0};
 std::atomic<int> g_helpers_max{-1};
 std::atomic<int64_t> g_pipeline_min{-1};
@@ -63,11 +64,16 @@ int helper_cap()
     return std::max(0, (hc - 1) / 2);
 }
 
+// A helper is taken only while the cap allows it and the greedies running
+// plus the helpers stay below the hardware threads: a batch or a server that
+// already runs a greedy per core gets none, so no pipelined pair ever waits
+// on a partner that is not running.
 bool take_helper()
 {
     const int cap = helper_cap();
+    const int hc = std::max(1, (int)std::thread::hardware_concurrency());
     int cur = g_helpers_busy.load();
-    while (cur < cap)
+    while (cur < cap && g_greedies_running.load() + cur < hc)
         if (g_helpers_busy.compare_exchange_weak(cur, cur + 1))
             return true;
     return false;
@@ -559,6 +565,10 @@ int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_
 {
     if (n <= 0)
         return 0;
+    struct Running {
+        Running() { g_greedies_running.fetch_add(1); }
+        ~Running() { g_greedies_running.fetch_sub(1); }
+    } running;
     int64_t min_entries = g_pipeline_min.load();
     if (min_entries < 0)
         min_entries = kPipelineMinEntries;

@@ -102,26 +102,32 @@ def test_two_threads_reference_fixtures(G):
 
 
 def test_concurrent_greedies_share_a_helper(G, oracle):
-    """Six greedies at once with one helper thread allowed: some run
-    two-threaded, the rest single-threaded; every result is the oracle's."""
+    """Several greedies at once with one helper thread allowed: at most one
+    runs two-threaded (a helper is granted only while the greedies running
+    plus the helpers stay below the hardware threads), the rest
+    single-threaded; every result is the oracle's."""
+    import os
+
     n, (rp, cols) = graphs()["wrap"]
     want = oracle.codebook(rp, cols, n, 1)
     G.set_greedy_threads(1, 0)
     p0, s0 = G.greedy_stats()
-    results = [None] * 6
+    k = max(2, min(6, (os.cpu_count() or 2) - 2))
+    results = [None] * k
 
     def run(k):
         results[k] = G.codebook_from_upper_csr(rp, cols, n, 1)
 
-    ts = [threading.Thread(target=run, args=(k,)) for k in range(6)]
+    ts = [threading.Thread(target=run, args=(q,)) for q in range(k)]
     for t in ts:
         t.start()
     for t in ts:
         t.join()
     p1, s1 = G.greedy_stats()
     G.set_greedy_threads(-1, -1)
-    assert (p1 - p0) + (s1 - s0) == 6
-    assert p1 - p0 >= 1
+    assert (p1 - p0) + (s1 - s0) == k
+    if (os.cpu_count() or 1) >= k + 2:
+        assert p1 - p0 >= 1
     for r in results:
         assert np.array_equal(r, want)
 
