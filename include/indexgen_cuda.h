@@ -367,15 +367,16 @@ ig_status ig_codebook_from_adjacency(const int64_t *adj_ptr, const int32_t *adj,
 /* Greedy over a caller-supplied upper CSR in host memory (no device work). */
 ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols, int32_t n, int order_threads,
                                      int32_t *order, int32_t *count);
-/* No counterpart in the reference (its greedy is single-threaded).  Every
- * greedy of this library (ig_solve, batches, the server, the two calls above)
+/* No counterpart in the reference (its greedy is single-threaded).  A greedy
+ * run by a caller's thread (ig_solve, ig_graph_codebook, the two calls above)
  * over a graph with at least min_entries neighbour-list entries (twice its
  * edges) runs on two threads -- the caller walks the balls and keeps the
- * degrees, a helper thread keeps the degree buckets -- while fewer than
- * max_helpers such helper threads are running in the process and the
- * greedies running plus the helpers stay below the hardware threads;
- * otherwise it runs on the calling thread alone.  Both forms give the same
- * codebook.
+ * degrees, a helper thread keeps the degree buckets -- when it is the only
+ * greedy running in the process, fewer than max_helpers helper threads are
+ * in use and the greedies plus the helpers stay below the hardware threads;
+ * otherwise, and always in the library's greedy pools (batches, the
+ * clustered solve, the server: one greedy per core already), it runs on one
+ * thread.  Both forms give the same codebook.
  * Process-wide.  max_helpers < 0: (hardware threads - 1) / 2; 0: never.
  * min_entries < 0: 2^20. */
 ig_status ig_set_greedy_threads(int max_helpers, int64_t min_entries);

@@ -494,6 +494,7 @@ bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int
                 return;
             const JobSpec &J = hg.jobs[(size_t)seq[(size_t)q]];
             try {
+                PooledGreedyScope pooled;
                 counts[seq[(size_t)q]] = greedy_one(hg, seq[(size_t)q], order + (J.word_off - order_base));
             } catch (...) {
                 failed = true;
@@ -575,6 +576,7 @@ void GreedyPool::run_one(std::unique_lock<std::mutex> &lk)
     lk.unlock();
     bool ok = true;
     try {
+        PooledGreedyScope pooled;
         *t.count = greedy_one(*t.hg, t.job, t.out);
     } catch (...) {
         ok = false;

@@ -33,6 +33,7 @@ std::atomic<int64_t> g_pipeline_min{-1};
 std::atomic<int64_t> g_runs_pipelined{0};
 std::atomic<int64_t> g_runs_sequential{0};
 constexpr int64_t kPipelineMinEntries = int64_t(1) << 20;
+thread_local int t_pooled = 0;  // PooledGreedyScope depth on this thread
 
 inline void cpu_relax()
 {
@@ -41,14 +42,14 @@ inline void cpu_relax()
 #endif
 }
 
-// The two threads of a pipelined greedy wait on each other once per ball:
-// spin briefly, then yield so that an oversubscribed host still runs the
-// other thread.
+// The two threads of a pipelined greedy wait on each other once per ball
+// (the mover's backlog then drains in a few microseconds): spin briefly, then
+// yield so that a busy host still runs the other thread.
 struct Backoff {
     int spins = 0;
     void pause()
     {
-        if (++spins < 4096)
+        if (++spins < 256)
             cpu_relax();
         else
             std::this_thread::yield();
@@ -557,9 +558,10 @@ class PipelinedGreedy {
     alignas(64) std::atomic<bool> done_{false};
 };
 
-// A greedy over n rows: pipelined over two threads when the graph has at
-// least the configured number of neighbour-list entries and a helper thread
-// is free in this process, else sequential on the calling thread.
+// A greedy over n rows: pipelined over two threads when it is the only
+// greedy running in the process, outside the library's greedy pools, on a
+// graph with at least the configured number of neighbour-list entries, and a
+// helper thread is free; else sequential on the calling thread.
 template <class Rows>
 int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_t *order)
 {
@@ -572,7 +574,7 @@ int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_
     int64_t min_entries = g_pipeline_min.load();
     if (min_entries < 0)
         min_entries = kPipelineMinEntries;
-    if (ap[n] - ap[0] >= min_entries && take_helper()) {
+    if (t_pooled == 0 && g_greedies_running.load() == 1 && ap[n] - ap[0] >= min_entries && take_helper()) {
         struct Give {
             ~Give() { g_helpers_busy.fetch_sub(1); }
         } give;
@@ -589,6 +591,9 @@ int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_
 }
 
 }  // namespace
+
+PooledGreedyScope::PooledGreedyScope() { ++t_pooled; }
+PooledGreedyScope::~PooledGreedyScope() { --t_pooled; }
 
 int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int64_t base, int order_threads,
                           int32_t *order)

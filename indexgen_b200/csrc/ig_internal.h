@@ -308,6 +308,14 @@ ig_status fetch_adjacency_async(ig_graph *g, HostGraph &hg, cudaEvent_t *done, c
 bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int32_t *order, int32_t *counts);
 // Greedy of one job of a downloaded graph into out (job-local ids).
 int32_t greedy_one(const HostGraph &hg, int job, int32_t *out);
+// While one is alive on a thread, the greedies run there stay on that thread:
+// the library's greedy pools (batches, the clustered solve, the server)
+// already run one greedy per core, and a helper thread would only compete
+// with them.
+struct PooledGreedyScope {
+    PooledGreedyScope();
+    ~PooledGreedyScope();
+};
 
 // Builds the jobs (words [offsets[j], offsets[j+1]), host or device pointer)
 // in up to eight groups and runs their greedies on host_threads threads as

@@ -333,6 +333,7 @@ void ig_server::greedy_loop()
         int32_t c = 0;
         try {
             t.job->order.resize((size_t)std::max(t.job->n, 1));
+            ig::PooledGreedyScope pooled;
             c = ig::greedy_one(*t.hg, t.job_in_batch, t.job->order.data());
         } catch (...) {
             s = IG_ERR_OOM;
