@@ -487,6 +487,11 @@ bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int
     });
     std::atomic<int> next{0};
     std::atomic<bool> failed{false};
+    int T = host_threads > 0 ? host_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    T = std::max(1, std::min(T, k));
+    // several threads: a pool, one greedy per thread; one: the caller's own
+    // greedies, one after another
+    const bool pooled = T > 1;
     auto worker = [&]() {
         for (;;) {
             const int q = next++;
@@ -494,15 +499,13 @@ bool run_greedies(const HostGraph &hg, int host_threads, int64_t order_base, int
                 return;
             const JobSpec &J = hg.jobs[(size_t)seq[(size_t)q]];
             try {
-                PooledGreedyScope pooled;
+                PooledGreedyScope scope(pooled);
                 counts[seq[(size_t)q]] = greedy_one(hg, seq[(size_t)q], order + (J.word_off - order_base));
             } catch (...) {
                 failed = true;
             }
         }
     };
-    int T = host_threads > 0 ? host_threads : (int)std::max(1u, std::thread::hardware_concurrency());
-    T = std::max(1, std::min(T, k));
     if (T == 1) {
         worker();
     } else {

@@ -592,8 +592,17 @@ int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_
 
 }  // namespace
 
-PooledGreedyScope::PooledGreedyScope() { ++t_pooled; }
-PooledGreedyScope::~PooledGreedyScope() { --t_pooled; }
+PooledGreedyScope::PooledGreedyScope(bool on) : on_(on)
+{
+    if (on_)
+        ++t_pooled;
+}
+
+PooledGreedyScope::~PooledGreedyScope()
+{
+    if (on_)
+        --t_pooled;
+}
 
 int32_t greedy_from_upper(const int64_t *row_ptr, const int32_t *cols, int32_t n, int64_t base, int order_threads,
                           int32_t *order)

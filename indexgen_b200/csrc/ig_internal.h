@@ -313,8 +313,13 @@ int32_t greedy_one(const HostGraph &hg, int job, int32_t *out);
 // already run one greedy per core, and a helper thread would only compete
 // with them.
 struct PooledGreedyScope {
-    PooledGreedyScope();
+    explicit PooledGreedyScope(bool on = true);
     ~PooledGreedyScope();
+    PooledGreedyScope(const PooledGreedyScope &) = delete;
+    PooledGreedyScope &operator=(const PooledGreedyScope &) = delete;
+
+  private:
+    bool on_;
 };
 
 // Builds the jobs (words [offsets[j], offsets[j+1]), host or device pointer)
