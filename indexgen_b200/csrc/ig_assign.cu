@@ -30,11 +30,23 @@ using myers::row_pools;
 constexpr int kAssignThreads = 256;
 constexpr int kCentreChunk = 2048;  // centre pools per shared-memory pass (16 KiB)
 
-template <int L>
+// The running minimum of the two-lane form as one key per word: distance in
+// bits 26..30, centre index in bits 0..25, so one unsigned min keeps the
+// nearest centre and, among equals, the lowest index (np.argmin's first
+// occurrence).  The key is formed by two IMADs on the FMA pipe from the two
+// popcounts, with the multipliers 2^26 and -2^26 passed in as arguments so
+// that they stay multiplies; the ALU pipe, which the recurrence saturates,
+// then spends one min per distance instead of an add, a compare and two
+// selects.
+constexpr int kKeyShift = 26;
+constexpr uint32_t kKeyIndexMask = (1u << kKeyShift) - 1u;
+
+template <int L, bool kKeyed>
 __global__ void __launch_bounds__(kAssignThreads) assign_kernel(const uint32_t *__restrict__ words, long long n,
                                                                const uint32_t *__restrict__ centres, int k,
                                                                int32_t *__restrict__ out, uint32_t one,
-                                                               uint32_t two, uint32_t hi)
+                                                               uint32_t two, uint32_t hi, uint32_t unit,
+                                                               uint32_t neg_unit)
 {
     __shared__ uint2 pools[kCentreChunk];
     using U = Unit<L>;
@@ -56,6 +68,7 @@ __global__ void __launch_bounds__(kAssignThreads) assign_kernel(const uint32_t *
             sel[j] = 0u;
     }
     int best0 = INT_MAX, best1 = INT_MAX, arg0 = 0, arg1 = 0;
+    uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu;  // kKeyed: two-lane form, k <= 2^26
     for (int c0 = 0; c0 < k; c0 += kCentreChunk) {
         const int cn = min(kCentreChunk, k - c0);
         __syncthreads();  // the previous pass is done with the pools
@@ -68,15 +81,30 @@ __global__ void __launch_bounds__(kAssignThreads) assign_kernel(const uint32_t *
         for (int i = 0; i < cn; ++i) {
             const uint2 p = pools[i];
             if constexpr (U::kTwo) {
-                int d0, d1;
-                myers::myers_two_dist<L>(p.x, p.y, sel, one, two, d0, d1);
-                if (d0 < best0) {
-                    best0 = d0;
-                    arg0 = c0 + i;
-                }
-                if (d1 < best1) {
-                    best1 = d1;
-                    arg1 = c0 + i;
+                if constexpr (kKeyed) {
+                    uint32_t pv, mv;
+                    myers::myers_two_vectors<L>(p.x, p.y, sel, one, two, pv, mv);
+                    constexpr uint32_t M0 = (1u << L) - 1u;
+                    constexpr uint32_t M1 = M0 << 16;
+                    // (L + popc(Pv) - popc(Mv)) << 26 | index, modulo 2^32
+                    const uint32_t base = ((uint32_t)L << kKeyShift) + (uint32_t)(c0 + i);
+                    const uint32_t k0 = myers::imad((uint32_t)__popc(mv & M0), neg_unit,
+                                                    myers::imad((uint32_t)__popc(pv & M0), unit, base));
+                    const uint32_t k1 = myers::imad((uint32_t)__popc(mv & M1), neg_unit,
+                                                    myers::imad((uint32_t)__popc(pv & M1), unit, base));
+                    key0 = min(key0, k0);
+                    key1 = min(key1, k1);
+                } else {
+                    int d0, d1;
+                    myers::myers_two_dist<L>(p.x, p.y, sel, one, two, d0, d1);
+                    if (d0 < best0) {
+                        best0 = d0;
+                        arg0 = c0 + i;
+                    }
+                    if (d1 < best1) {
+                        best1 = d1;
+                        arg1 = c0 + i;
+                    }
                 }
             } else {
                 uint32_t s8[8];
@@ -91,20 +119,39 @@ __global__ void __launch_bounds__(kAssignThreads) assign_kernel(const uint32_t *
             }
         }
     }
+    if constexpr (kKeyed) {
+        arg0 = (int)(key0 & kKeyIndexMask);
+        arg1 = (int)(key1 & kKeyIndexMask);
+    }
     if (first < n)
         out[first] = arg0;
     if (U::kTwo && first + 1 < n)
         out[first + 1] = arg1;
 }
 
+// The keyed minimum for the two-lane lengths (L <= 15) with at most 2^26
+// centres; the compare-and-select form otherwise.
+template <int L>
+void launch_assign_len(int grid, cudaStream_t st, const uint32_t *words, long long n, const uint32_t *centres, int k,
+                       int32_t *out)
+{
+    constexpr uint32_t unit = 1u << kKeyShift;
+    if constexpr (Unit<L>::kTwo) {
+        if (k <= (int)kKeyIndexMask + 1) {
+            assign_kernel<L, true><<<grid, kAssignThreads, 0, st>>>(words, n, centres, k, out, 1u, 2u, 1u << 16,
+                                                                    unit, 0u - unit);
+            return;
+        }
+    }
+    assign_kernel<L, false><<<grid, kAssignThreads, 0, st>>>(words, n, centres, k, out, 1u, 2u, 1u << 16, unit,
+                                                             0u - unit);
+}
+
 template <int... Ls>
 void launch_assign(int L, int grid, cudaStream_t st, const uint32_t *words, long long n, const uint32_t *centres,
                    int k, int32_t *out, std::integer_sequence<int, Ls...>)
 {
-    ((L == Ls + 1 ? (void)(assign_kernel<Ls + 1><<<grid, kAssignThreads, 0, st>>>(words, n, centres, k, out, 1u, 2u,
-                                                                                  1u << 16))
-                  : void()),
-     ...);
+    ((L == Ls + 1 ? launch_assign_len<Ls + 1>(grid, st, words, n, centres, k, out) : void()), ...);
 }
 
 __global__ void gather_words_kernel(const uint32_t *__restrict__ src, const int32_t *__restrict__ idx, long long n,
