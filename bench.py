@@ -266,6 +266,31 @@ def profile_traffic(wl_name):
     return None
 
 
+def profile_path_traffic(wl_name):
+    """dram bytes per build of the whole device path (pair kernel, row
+    prefix, scan, scatter) from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"compaction_{wl_name}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("path_traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def path_traffic_line(wl_name, edges: int, n: int):
+    """The device path's measured DRAM bytes per build against 16 B per edge
+    + 20 B per row (each edge written once as a record and read once)."""
+    t = profile_path_traffic(wl_name)
+    plan = 16 * edges + 20 * n
+    return {"bytes_per_build": t, "bytes_per_edge": (t / edges) if t and edges else None,
+            "plan_bytes_16E_20N": plan, "ratio_to_plan": (t / plan) if t else None,
+            "source": f"profiles/compaction_{wl_name}.md (ncu dram__bytes_read + write, pair kernel to scatter)"}
+
+
 def touched_cells(n: int, seg_width: int, segments: int, band_rows: int = 256) -> int:
     """(row, segment) count cells the pair kernel writes and the compaction
     reads: a row's cells run from its band's first segment on (band_rows-row
@@ -930,6 +955,7 @@ def run_ours(args, wl, rank, world, dist):
                        "ms_per_launch": comp_avg_s * 1e3, "peak_source": f"{src} hbm_gbs",
                        "bytes_per_launch": comp_bytes, "count_cells": cells, "segment_width": seg_width,
                        "parts_ms_per_launch": comp_parts},
+        "path_traffic": path_traffic_line(wl["name"], edges, n),
         "gpu_launches": launches,
         "work_split": {"lane_form": ["full", "nibble", "byte"][lane_form(L, d)],
                        "items_per_cta": ctx.work_split(lane_form(L, d))[0],
