@@ -175,3 +175,32 @@ def test_two_threads_on_the_linear12_job(igctx):
     p1, s1 = greedy_stats()
     assert (p1, s1) == (p0, s0 + 1)
     assert np.array_equal(books[0], two)
+
+
+@pytest.mark.gpu
+def test_two_threads_on_batch_jobs_with_offsets(igctx):
+    """A batch graph's per-job codebooks computed on the caller's thread
+    alone (host_threads=1): each job's greedy is a lone greedy over rows whose
+    neighbour ids carry the job's word offset, in plain and in bit-packed
+    host lists.  With the two-thread form forced for every size, each equals
+    the job's own single-threaded solve."""
+    from indexgen_b200 import LISTS_AUTO, LISTS_PACKED, build_batch, greedy_stats, set_greedy_threads, solve
+    from indexgen_b200 import workloads as W
+
+    jobs = [(W.uniform_words(6000, 10, 41), 10, 4), (W.uniform_words(20000, 10, 42), 10, 5),
+            (W.uniform_words(9000, 12, 43), 12, 4)]
+    try:
+        set_greedy_threads(0, -1)
+        want = [solve(w, L, d, 1, igctx)[0] for w, L, d in jobs]
+        for lists in (LISTS_AUTO, LISTS_PACKED):
+            igctx.set_host_lists(lists)
+            set_greedy_threads(1, 0)
+            p0 = greedy_stats()[0]
+            with build_batch(jobs, igctx) as G:
+                books = G.job_codebooks(order_threads=1, host_threads=1)
+            assert greedy_stats()[0] == p0 + len(jobs)
+            for got, ref in zip(books, want):
+                assert np.array_equal(got, ref)
+    finally:
+        igctx.set_host_lists(LISTS_AUTO)
+        set_greedy_threads(-1, -1)
