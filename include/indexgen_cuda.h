@@ -373,9 +373,10 @@ ig_status ig_codebook_from_upper_csr(const int64_t *row_ptr, const int32_t *cols
  * edges) runs on two threads -- the caller walks the balls and keeps the
  * degrees, a helper thread keeps the degree buckets -- when it is the only
  * greedy running in the process, fewer than max_helpers helper threads are
- * in use and the greedies plus the helpers stay below the hardware threads;
- * otherwise, and always in the library's greedy pools (batches, the
- * clustered solve, the server: one greedy per core already), it runs on one
+ * in use and the greedies plus the helpers stay below the hardware threads.
+ * In the library's greedy pools (batches, the clustered solve, the server:
+ * one greedy per core already) only graphs with at least 64 * min_entries
+ * entries do so, under the same helper rule.  Otherwise a greedy runs on one
  * thread.  Both forms give the same codebook.
  * Process-wide.  max_helpers < 0: (hardware threads - 1) / 2; 0: never.
  * min_entries < 0: 2^20. */

@@ -558,10 +558,14 @@ class PipelinedGreedy {
     alignas(64) std::atomic<bool> done_{false};
 };
 
-// A greedy over n rows: pipelined over two threads when it is the only
-// greedy running in the process, outside the library's greedy pools, on a
-// graph with at least the configured number of neighbour-list entries, and a
-// helper thread is free; else sequential on the calling thread.
+// A greedy over n rows: pipelined over two threads when a helper thread is
+// free and either it is the only greedy running in the process, outside the
+// library's greedy pools, on a graph with at least the configured number of
+// neighbour-list entries, or it runs in a pool on a graph with 64 times that
+// (2^26 entries by default: the densest jobs of a stream, whose greedies run
+// for seconds to minutes while the small jobs' greedies come and go; the
+// helper rule keeps the greedies plus helpers below the hardware threads);
+// else sequential on the calling thread.
 template <class Rows>
 int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_t *order)
 {
@@ -574,7 +578,10 @@ int32_t run_greedy(const int64_t *ap, Rows rows, int32_t n, int64_t base, int32_
     int64_t min_entries = g_pipeline_min.load();
     if (min_entries < 0)
         min_entries = kPipelineMinEntries;
-    if (t_pooled == 0 && g_greedies_running.load() == 1 && ap[n] - ap[0] >= min_entries && take_helper()) {
+    const int64_t entries = ap[n] - ap[0];
+    const bool lone = t_pooled == 0 && g_greedies_running.load() == 1 && entries >= min_entries;
+    const bool large_pooled = t_pooled > 0 && entries / 64 >= min_entries;
+    if ((lone || large_pooled) && take_helper()) {
         struct Give {
             ~Give() { g_helpers_busy.fetch_sub(1); }
         } give;

@@ -204,3 +204,28 @@ def test_two_threads_on_batch_jobs_with_offsets(igctx):
     finally:
         igctx.set_host_lists(LISTS_AUTO)
         set_greedy_threads(-1, -1)
+
+
+@pytest.mark.gpu
+def test_large_pooled_greedy_takes_a_free_helper(igctx):
+    """In the library's greedy pool only graphs with at least 64 times the
+    lone threshold of entries run two-threaded (the densest jobs of a
+    stream); with the threshold lowered, a batch's dense job does, a small
+    one does not, and both codebooks equal their single-threaded solves."""
+    from indexgen_b200 import greedy_stats, set_greedy_threads, solve, solve_batch
+    from indexgen_b200 import workloads as W
+
+    dense = (W.uniform_words(20000, 10, 42), 10, 5)   # about 9e6 edges
+    small = (W.uniform_words(3000, 12, 44), 12, 3)    # a few hundred edges
+    try:
+        set_greedy_threads(0, -1)
+        want = [solve(w, L, d, 1, igctx)[0] for w, L, d in (dense, small)]
+        set_greedy_threads(1, 1 << 14)  # pooled threshold 2^20 entries
+        p0, s0 = greedy_stats()
+        books, _ = solve_batch([dense, small], 1, 0, igctx)
+        p1, s1 = greedy_stats()
+    finally:
+        set_greedy_threads(-1, -1)
+    assert (p1 - p0, s1 - s0) == (1, 1)
+    for got, ref in zip(books, want):
+        assert np.array_equal(got, ref)
